@@ -1,0 +1,169 @@
+/*
+ * jet_b200.h -- C ABI of the B200 Jet multilevel k-way graph partitioner.
+ *
+ * Plain pointers and sizes only.  Every entry point returns a status code
+ * (JET_OK on success).  Graph arrays describe a symmetric CSR without
+ * self-loops with both edge directions stored, as the reference's
+ * KokkosSparse::CrsMatrix input does (header/jet_defs.h:64-92):
+ *   row_map[n+1]  edge offsets       entries[nnz]  neighbour ids
+ *   values[nnz]   edge weights       vweights[n]   vertex weights
+ * Three integer tiers mirror header/jet_defs.h:47-92:
+ *   _i32      int32 ordinals, int32 offsets, int32 weights   (jet.h "std")
+ *   _big      int32 ordinals, int64 offsets, int64 weights
+ *   _biggest  int64 ordinals, int64 offsets, int64 weights
+ * Part ids are int32.  `mem` says where the graph and output arrays live:
+ * JET_MEM_HOST (the library copies in and out) or JET_MEM_DEVICE (pointers
+ * into the current CUDA device's memory).  `stream` is a cudaStream_t (NULL =
+ * the library's own stream); calls return after the result is written.
+ */
+#ifndef JET_B200_H
+#define JET_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    JET_OK = 0,
+    JET_ERR_INVALID = 1,   /* bad argument or malformed graph */
+    JET_ERR_CUDA = 2,      /* CUDA runtime error */
+    JET_ERR_METIS = 3,     /* Metis failed on the coarsest graph (the reference exits) */
+    JET_ERR_OOM = 4,       /* device allocation failed */
+    JET_ERR_OVERFLOW = 5,  /* a hash table ran out of room */
+    JET_ERR_TIMEOUT = 6,   /* a bounded device loop gave up */
+    JET_ERR_NOT_BUILT = 7  /* no CUDA device / library not usable */
+};
+
+enum { JET_MEM_HOST = 0, JET_MEM_DEVICE = 1 };
+
+/* config_t of header/jet_config.h:43-52, field for field. */
+typedef struct jet_config_c {
+    int32_t coarsening_alg;   /* 0 = 2-hop matching, 1 = HEC, 2 = pure matching */
+    int32_t num_iter;         /* used by drivers only (attempt count) */
+    double max_imb_ratio;
+    int32_t num_parts;
+    double refine_tolerance;  /* default 0.999 */
+    int32_t dump_coarse;      /* accepted, ignored (experiment dump) */
+    int32_t verbose;
+    int32_t ultra_settings;
+} jet_config_c;
+
+/* experiment_data<...>::CoarseLevel, header/experiment_data.hpp:102-123. */
+typedef struct jet_level_stats_c {
+    int64_t edge_cut;
+    double imb;
+    uint64_t num_edges;
+    uint64_t num_vertices;
+    double total_ref_time;
+    double iterations_time;
+    int32_t total_iterations;
+    int32_t lp_iterations;
+} jet_level_stats_c;
+
+#define JET_MAX_LEVELS 256
+#define JET_NUM_MEASUREMENTS 20
+
+/* experiment_data<...>, header/experiment_data.hpp:76-175.  measurements[]
+ * follows the Measurement enum order (coarsen-map ... total), in seconds. */
+typedef struct jet_stats_c {
+    double measurements[JET_NUM_MEASUREMENTS];
+    int32_t num_levels;
+    jet_level_stats_c levels[JET_MAX_LEVELS]; /* coarsest first, as refined */
+    int64_t edge_cut;        /* final cut, each cut edge once */
+    int64_t max_part_cut;    /* filled when verbose */
+    int64_t objective;       /* communication volume, filled when verbose */
+    double imb_ratio;        /* largest part / optimal size */
+    int64_t largest_part;
+    int64_t smallest_part;
+    int64_t coarsest_vertices;
+    int64_t refine_iterations;
+} jet_stats_c;
+
+/* ---------------------------------------------------------------- partition
+ * Replaces jet_partitioner::partition / partition_big / partition_biggest
+ * (header/jet.h:46-51, :67-72, :88-93; bodies src/jet.cpp:47-54,
+ * src/jet_big.cpp:47-54, src/jet_biggest.cpp:47-54): coarsen, Metis on the
+ * coarsest graph, uncoarsen with Jet refinement.  part_out[n] receives the
+ * partition, *edge_cut the cut (each edge once).  `seed` drives the
+ * coarsening RNG (the reference seeds from the clock). stats may be NULL. */
+int jet_partition_i32(const jet_config_c* config, int32_t n, const int32_t* row_map, const int32_t* entries,
+                      const int32_t* values, const int32_t* vweights, int uniform_ew, int mem, uint64_t seed,
+                      void* stream, int32_t* part_out, int32_t* edge_cut, jet_stats_c* stats);
+int jet_partition_big(const jet_config_c* config, int32_t n, const int64_t* row_map, const int32_t* entries,
+                      const int64_t* values, const int64_t* vweights, int uniform_ew, int mem, uint64_t seed,
+                      void* stream, int32_t* part_out, int64_t* edge_cut, jet_stats_c* stats);
+int jet_partition_biggest(const jet_config_c* config, int64_t n, const int64_t* row_map, const int64_t* entries,
+                          const int64_t* values, const int64_t* vweights, int uniform_ew, int mem, uint64_t seed,
+                          void* stream, int32_t* part_out, int64_t* edge_cut, jet_stats_c* stats);
+
+/* ---------------------------------------------------------------- components
+ * Tier-generic entry points over device pointers (tier 0 = i32, 1 = big,
+ * 2 = biggest; pointer element types follow the tier).  They expose the hot
+ * path's stages one at a time. */
+
+/* One coarsening map (src/contract.hpp:448-492): alg 0 = 2-hop matching
+ * (src/heuristics.hpp:427-671 with match_choice 1), 1 = HEC
+ * (src/heuristics.hpp:171-262), 2 = pure matching.  map_out[n] receives the
+ * fine->coarse map, hn_out[n] (nullable) the initial heavy-neighbour
+ * proposals, *nc the coarse vertex count. */
+int jet_coarsen_map(int tier, int alg, int level, uint64_t seed, int64_t n, int64_t nnz, const void* row_map,
+                    const void* entries, const void* values, const void* vweights, int uniform, void* map_out,
+                    void* hn_out, int64_t* nc, void* stream);
+
+/* Contraction under a given map (src/contract.hpp:347-446): crow[nc+1],
+ * cadj[>= nnz], cval[>= nnz], cvw[nc]; *cnnz receives the coarse nnz.  Row
+ * order within a coarse row is unspecified. */
+int jet_contract(int tier, int64_t n, int64_t nnz, const void* row_map, const void* entries, const void* values,
+                 const void* vweights, const void* map, int64_t nc, void* crow, void* cadj, void* cval, void* cvw,
+                 int64_t* cnnz, void* stream);
+
+/* Connectivity tables for a partition (init_conn_data,
+ * src/jet_refiner.hpp:958-1048): off[n+1], ent[>= nnz] (part or -1/-2),
+ * val[>= nnz], size[n]. */
+int jet_conn_build(int tier, int64_t n, int64_t nnz, const void* row_map, const void* entries, const void* values,
+                   const int32_t* part, int32_t k, void* off, int32_t* ent, void* val, int32_t* size, void* stream);
+
+/* `iters` refinement iterations at one level from part[] (in/out) with the
+ * iteration body of jet_refine (src/jet_refiner.hpp:1106-1120) and no
+ * best-state bookkeeping.  sizes[k], *cut (both directions), the tables as
+ * jet_conn_build, dest_cache[n], and per iteration moves[i] and kinds[i]
+ * (0 LP, 1 weak, 2 strong).  Table outputs may be NULL. */
+int jet_refine_iters(int tier, int64_t n, int64_t nnz, const void* row_map, const void* entries, const void* values,
+                     const void* vweights, int32_t* part, int32_t k, double imb, double filter_ratio, int32_t iters,
+                     void* sizes, int64_t* cut, void* off, int32_t* ent, void* val, int32_t* size, int32_t* dest_cache,
+                     int64_t* moves, int32_t* kinds, void* stream);
+
+/* One full jet_refine at a single level (src/jet_refiner.hpp:1050-1142):
+ * part[] in/out, *cut (both directions), *iters. */
+int jet_refine_level(int tier, int64_t n, int64_t nnz, const void* row_map, const void* entries, const void* values,
+                     const void* vweights, int32_t* part, int32_t k, double imb, double tol, int uniform_ew,
+                     int64_t* cut, int32_t* iters, void* stream);
+
+/* Partition quality as pstat reports it (app/part_eval.cpp:73-110):
+ * out[6] = {cut (each edge once), max part cut, comm size, largest part,
+ * smallest part, total vertex weight}. */
+int jet_pstat(int tier, int64_t n, int64_t nnz, const void* row_map, const void* entries, const void* values,
+              const void* vweights, const int32_t* part, int32_t k, int64_t* out, void* stream);
+
+/* Projection to the finer level (src/uncoarsen.hpp:82-86): fine[i] = coarse[map[i]]. */
+int jet_project(int tier, int64_t n_fine, const void* map, const int32_t* coarse, int32_t* fine, void* stream);
+
+/* ---------------------------------------------------------------- runtime
+ * Library version string, last error message (thread-local), device sanity. */
+const char* jet_version(void);
+const char* jet_last_error(void);
+int jet_device_ok(void);
+
+/* Kernel-class timing with CUDA events on the launching stream (used by the
+ * benchmark).  kinds: 0 conn build, 1 LP select, 2 afterburner, 3 table
+ * updates, 4 contraction, 5 heavy-edge proposal.  jet_prof_read fills
+ * ms[6], bytes[6] (algorithmic bytes), launches[6]. */
+int jet_prof_enable(int on);
+int jet_prof_read(double* ms, double* bytes, int64_t* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,379 @@
+// partitioner.cuh -- host orchestration: coarsening level loop, Metis on the
+// coarsest graph, uncoarsening with Jet refinement and projection.
+// Mirrors src/partitioner.hpp, src/contract.hpp:448-533,
+// src/uncoarsen.hpp:88-158 and src/jet_refiner.hpp:1050-1142.
+#pragma once
+#include <chrono>
+#include <vector>
+#include <memory>
+#include "coarsen.cuh"
+#include "contract.cuh"
+#include "refine.cuh"
+#include "../../include/jet_b200.h"
+
+typedef int64_t metis_idx_t;
+typedef float metis_real_t;
+// Public METIS 5 API (this build's library uses 64-bit idx_t, float real_t).
+extern "C" int METIS_PartGraphKway(metis_idx_t*, metis_idx_t*, metis_idx_t*, metis_idx_t*, metis_idx_t*, metis_idx_t*,
+                                   metis_idx_t*, metis_idx_t*, metis_real_t*, metis_real_t*, metis_idx_t*, metis_idx_t*,
+                                   metis_idx_t*);
+
+namespace jetb {
+
+struct JetError {
+    int code;
+    const char* what;
+};
+
+using clk = std::chrono::steady_clock;
+inline double since(clk::time_point a) { return std::chrono::duration<double>(clk::now() - a).count(); }
+
+// Measurement slots, header/experiment_data.hpp:50-72.
+enum Meas { M_MAP = 0, M_BUILD, M_COUNT, M_PREFIX, M_BUCKET, M_DEDUPE, M_RADIXSORT, M_RADIXDEDUPE, M_WRITEGRAPH, M_PERMUTE,
+            M_MAPCONSTRUCT, M_HEAVY, M_INITTRANSFER, M_HASHMAPALLOC, M_HASHMAPINSERT, M_INITPARTITION, M_COARSEN, M_REFINE,
+            M_FREEGRAPH, M_TOTAL };
+
+template <class O, class E, class W>
+struct Engine {
+    cudaStream_t s;
+    ScanScratch scan;
+    DBuf<int64_t> dscal;   // small device scalars
+    int64_t* hscal = nullptr;  // pinned mirror
+    IterResult* hres = nullptr;
+    int seed_level_base = 0;
+
+    explicit Engine(cudaStream_t st) : s(st) {
+        dscal.alloc(64, s);
+        JET_CUDA(cudaHostAlloc((void**)&hscal, 64 * sizeof(int64_t), cudaHostAllocMapped));
+        JET_CUDA(cudaHostAlloc((void**)&hres, sizeof(IterResult), cudaHostAllocMapped));
+    }
+    ~Engine() {
+        cudaStreamSynchronize(s);
+        if (hscal) cudaFreeHost(hscal);
+        if (hres) cudaFreeHost(hres);
+    }
+    template <class T> T* dslot(int i) { return (T*)(dscal.p + i); }
+    void sync() { JET_CUDA(cudaStreamSynchronize(s)); }
+    // copies `cnt` device scalars starting at slot 0 to the host mirror
+    void pull(int cnt) {
+        JET_CUDA(cudaMemcpyAsync(hscal, dscal.p, sizeof(int64_t) * cnt, cudaMemcpyDeviceToHost, s));
+        sync();
+    }
+
+    // ------------------------------------------------------------ level prep
+    void prepare_level(Level<O, E, W>& L) {
+        L.warp_list.alloc(L.n > 0 ? L.n : 1, s);
+        L.hub_list.alloc(L.n > 0 ? L.n : 1, s);
+        JET_CUDA(cudaMemsetAsync(dscal.p, 0, 3 * sizeof(int64_t), s));
+        if (L.n > 0) {
+            k_bin_degrees<O, E><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(L.n, L.row, L.warp_list.p, dslot<O>(0), L.hub_list.p,
+                                                                          dslot<O>(1), dslot<E>(2));
+            JET_LAUNCH_CHECK();
+        }
+        pull(3);
+        L.n_warp = *(O*)&hscal[0];
+        L.n_hub = *(O*)&hscal[1];
+        L.max_deg = *(E*)&hscal[2];
+        double avg = L.n > 0 ? (double)L.m / (double)L.n : 0.0;
+        L.group = group_for_avg_degree(avg);
+    }
+
+    // ------------------------------------------------------------ coarsening
+    O hec_map(Level<O, E, W>& L, uint64_t seed, int level, O* vcmap, O* hn_out, double* t_heavy, double* t_construct) {
+        auto g = L.view();
+        O n = L.n;
+        DBuf<O> hn_own;
+        O* hn = hn_out;
+        if (!hn) { hn_own.alloc(n, s); hn = hn_own.p; }
+        auto t0 = clk::now();
+        if (L.uniform) {
+            k_hec_uniform<O, E, W><<<grid_persistent(n, 16), BLOCK, 0, s>>>(g, seed, rng_stream(level, RNG_HEC_RANDOM, 0), hn);
+            JET_LAUNCH_CHECK();
+        } else {
+            W* vsum = dslot<W>(8);
+            JET_CUDA(cudaMemsetAsync(vsum, 0, sizeof(int64_t), s));
+            k_sum<W><<<grid_persistent(n, 8), BLOCK, 0, s>>>(g.vw, n, vsum);
+            JET_LAUNCH_CHECK();
+            unsigned grid = grid_persistent((int64_t)n * L.group, 16);
+            switch (L.group) {
+                case 4: k_hec_heavy<4, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); break;
+                case 8: k_hec_heavy<8, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); break;
+                case 16: k_hec_heavy<16, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); break;
+                default: k_hec_heavy<32, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); break;
+            }
+            JET_LAUNCH_CHECK();
+            if (L.n_hub > 0) {
+                k_hec_heavy_hub<O, E, W><<<grid_for(L.n_hub, 1), 1024, 0, s>>>(g, vsum, L.hub_list.p, L.n_hub, hn);
+                JET_LAUNCH_CHECK();
+            }
+        }
+        if (t_heavy) { sync(); *t_heavy += since(t0); }
+        auto t1 = clk::now();
+        fill<O>(vcmap, n, ord_max<O>(), s);
+        DBuf<O> perm_a(n, s), perm_b(n, s);
+        O* cur = nullptr;  // identity in the first round
+        O* nxt = perm_a.p;
+        O* cur_len = dslot<O>(16);
+        O* nxt_len = dslot<O>(17);
+        int swap = 1;
+        O len = n;
+        int rounds = 0;
+        while (len > 0) {
+            JET_CUDA(cudaMemsetAsync(nxt_len, 0, sizeof(int64_t), s));
+            unsigned grid = grid_persistent(len, 16);
+            k_hec_round<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn, vcmap, swap);
+            JET_LAUNCH_CHECK();
+            k_hec_compact<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, vcmap, nxt, nxt_len);
+            JET_LAUNCH_CHECK();
+            JET_CUDA(cudaMemcpyAsync(cur_len, nxt_len, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
+            JET_CUDA(cudaMemcpyAsync(hscal, nxt_len, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            sync();
+            len = *(O*)hscal;
+            swap ^= 1;
+            cur = nxt;
+            nxt = (nxt == perm_a.p) ? perm_b.p : perm_a.p;
+            if (++rounds > 100000) throw JetError{JET_ERR_TIMEOUT, "HEC aggregation did not settle"};
+        }
+        O nc = number_roots(vcmap, n);
+        if (t_construct) *t_construct += since(t1);
+        return nc;
+    }
+
+    O number_roots(O* vcmap, O n) {
+        DBuf<O> ids(n + 1, s);
+        O* total = dslot<O>(20);
+        exclusive_scan<O, GetIsRoot<O>>(GetIsRoot<O>{vcmap}, n, ids.p, total, scan, s);
+        k_assign_ids<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, ids.p, vcmap);
+        JET_LAUNCH_CHECK();
+        JET_CUDA(cudaMemcpyAsync(hscal, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        sync();
+        return *(O*)hscal;
+    }
+
+    template <bool INITIAL, bool UNIFORM>
+    void pick(Level<O, E, W>& L, const O* perm, const O* perm_len, O max_len, const O* vcmap, O* hn, uint64_t seed, uint64_t stream) {
+        auto g = L.view();
+        unsigned grid = grid_persistent((int64_t)max_len * L.group, 16);
+        switch (L.group) {
+            case 4: k_pick_match<4, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); break;
+            case 8: k_pick_match<8, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); break;
+            case 16: k_pick_match<16, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); break;
+            default: k_pick_match<32, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); break;
+        }
+        JET_LAUNCH_CHECK();
+        if (L.n_hub > 0) {
+            k_pick_match_hub<INITIAL, UNIFORM, O, E, W><<<grid_for(L.n_hub, 1), 1024, 0, s>>>(g, L.hub_list.p, L.n_hub, vcmap, hn, seed, stream);
+            JET_LAUNCH_CHECK();
+        }
+    }
+
+    // coarsen_match, src/heuristics.hpp:427-671.
+    O match_map(Level<O, E, W>& L, bool two_hop, uint64_t seed, int level, O* vcmap, O* hn_init_out) {
+        auto g = L.view();
+        O n = L.n;
+        const O MAXV = ord_max<O>();
+        DBuf<O> hn(n, s);
+        fill<O>(hn.p, n, MAXV, s);
+        fill<O>(vcmap, n, MAXV, s);
+        if (L.uniform) {
+            k_match_uniform_init<O, E, W><<<grid_persistent(n, 16), BLOCK, 0, s>>>(g, seed, rng_stream(level, RNG_MATCH_RANDOM, 0), hn.p);
+            JET_LAUNCH_CHECK();
+        } else {
+            pick<true, false>(L, nullptr, nullptr, n, vcmap, hn.p, seed, rng_stream(level, RNG_MATCH_PICK, 0));
+        }
+        if (hn_init_out) JET_CUDA(cudaMemcpyAsync(hn_init_out, hn.p, sizeof(O) * n, cudaMemcpyDeviceToDevice, s));
+        DBuf<O> perm_a(n, s), perm_b(n, s);
+        O* cur = nullptr;
+        O* cur_len = dslot<O>(16);
+        O* nxt_len = dslot<O>(17);
+        O len = n;
+        int outer = 0;
+        while (len > 0) {
+            unsigned grid = grid_persistent(len, 16);
+            for (int r = 0; r < 4; r++) {
+                k_commit1<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap, r);
+                k_commit2<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap);
+                k_commit3<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, vcmap);
+                JET_LAUNCH_CHECK();
+            }
+            outer++;
+            uint64_t st = rng_stream(level, RNG_MATCH_PICK, outer);
+            if (L.uniform) pick<false, true>(L, cur, cur_len, len, vcmap, hn.p, seed, st);
+            else pick<false, false>(L, cur, cur_len, len, vcmap, hn.p, seed, st);
+            O* nxt = (cur == perm_a.p) ? perm_b.p : perm_a.p;
+            JET_CUDA(cudaMemsetAsync(nxt_len, 0, sizeof(int64_t), s));
+            k_match_remaining<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap, nxt, nxt_len);
+            JET_LAUNCH_CHECK();
+            JET_CUDA(cudaMemcpyAsync(cur_len, nxt_len, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
+            JET_CUDA(cudaMemcpyAsync(hscal, nxt_len, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            sync();
+            len = *(O*)hscal;
+            cur = nxt;
+            if (outer > 100000) throw JetError{JET_ERR_TIMEOUT, "matching did not settle"};
+        }
+        if (two_hop) two_hop_passes(L, vcmap);
+        k_singletons<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, vcmap);
+        JET_LAUNCH_CHECK();
+        return number_roots(vcmap, n);
+    }
+
+    O count_unmatched(O n, const O* vcmap) {
+        O* c = dslot<O>(24);
+        JET_CUDA(cudaMemsetAsync(c, 0, sizeof(int64_t), s));
+        k_count_unmatched<O><<<grid_persistent(n, 8), BLOCK, 0, s>>>(n, vcmap, c);
+        JET_LAUNCH_CHECK();
+        JET_CUDA(cudaMemcpyAsync(hscal, c, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        sync();
+        return *(O*)hscal;
+    }
+
+    O unmatched_list(Level<O, E, W>& L, const O* vcmap, int leaves_only, DBuf<O>& list) {
+        O n = L.n;
+        DBuf<O> pos(n, s);
+        O* total = dslot<O>(25);
+        exclusive_scan<O, GetUnmatched<O, E>>(GetUnmatched<O, E>{vcmap, L.row, leaves_only}, n, pos.p, total, scan, s);
+        JET_CUDA(cudaMemcpyAsync(hscal, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        sync();
+        O cnt = *(O*)hscal;
+        list.alloc(cnt > 0 ? cnt : 1, s);
+        k_scatter_unmatched<O, E><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, vcmap, L.row, leaves_only, pos.p, list.p);
+        JET_LAUNCH_CHECK();
+        return cnt;
+    }
+
+    template <class H>
+    void match_hash(const O* list, const H* hashes, O mappable, H nullkey, O* vcmap) {
+        if (mappable <= 0) return;
+        DBuf<H> ht(mappable, s);
+        DBuf<O> twins(mappable, s);
+        fill<H>(ht.p, mappable, nullkey, s);
+        fill<O>(twins.p, mappable, (O)-1, s);
+        int* err = dslot<int>(30);
+        JET_CUDA(cudaMemsetAsync(err, 0, sizeof(int64_t), s));
+        k_match_hash<O, H><<<grid_persistent(mappable, 16), BLOCK, 0, s>>>(list, hashes, mappable, nullkey, ht.p, twins.p, vcmap, err);
+        JET_LAUNCH_CHECK();
+        JET_CUDA(cudaMemcpyAsync(hscal, err, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        sync();
+        if (*(int*)hscal) throw JetError{JET_ERR_TIMEOUT, "2-hop hash matching exceeded its probe bound"};
+    }
+
+    void two_hop_passes(Level<O, E, W>& L, O* vcmap) {
+        auto g = L.view();
+        O n = L.n;
+        const O MAXV = ord_max<O>();
+        O unmapped = count_unmatched(n, vcmap);
+        if ((double)unmapped / (double)n > 0.25) {  // leaves, src/heuristics.hpp:539-560
+            DBuf<O> list;
+            O cnt = unmatched_list(L, vcmap, 1, list);
+            if (cnt > 0) {
+                DBuf<O> hs(cnt, s);
+                k_leaf_hash<O, E, W><<<grid_persistent(cnt, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p);
+                JET_LAUNCH_CHECK();
+                match_hash<O>(list.p, hs.p, cnt, MAXV, vcmap);
+            }
+        }
+        unmapped = count_unmatched(n, vcmap);
+        if ((double)unmapped / (double)n > 0.25) {  // twins, src/heuristics.hpp:565-598
+            DBuf<O> list;
+            O cnt = unmatched_list(L, vcmap, 0, list);
+            if (cnt > 0) {
+                DBuf<uint64_t> hs(cnt, s);
+                k_twin_hash<O, E, W><<<grid_persistent((int64_t)cnt * 32, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p);
+                JET_LAUNCH_CHECK();
+                if (L.n_hub > 0) {
+                    k_twin_hash_hub<O, E, W><<<grid_for(cnt, 1) < 4096 ? grid_for(cnt, 1) : 4096, 1024, 0, s>>>(g, list.p, cnt, hs.p);
+                    JET_LAUNCH_CHECK();
+                }
+                match_hash<uint64_t>(list.p, hs.p, cnt, (uint64_t)0, vcmap);
+            }
+        }
+        unmapped = count_unmatched(n, vcmap);
+        if ((double)unmapped / (double)n > 0.25) {  // relatives, src/heuristics.hpp:603-640
+            DBuf<O> list;
+            O cnt = unmatched_list(L, vcmap, 0, list);
+            if (cnt > 0) {
+                DBuf<O> hs(cnt, s);
+                k_relative_hash<O, E, W><<<grid_persistent(cnt, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p);
+                JET_LAUNCH_CHECK();
+                match_hash<O>(list.p, hs.p, cnt, MAXV, vcmap);
+            }
+        }
+    }
+
+    // generate_coarse_mapping, src/contract.hpp:448-492.
+    O coarsen_map(Level<O, E, W>& L, int alg, uint64_t seed, int level, O* vcmap, O* hn_out, double* meas) {
+        if (alg == 1) return hec_map(L, seed, level, vcmap, hn_out, meas ? &meas[M_HEAVY] : nullptr, meas ? &meas[M_MAPCONSTRUCT] : nullptr);
+        return match_map(L, alg == 0, seed, level, vcmap, hn_out);
+    }
+
+    // ------------------------------------------------------------ contraction
+    // build_coarse_graph, src/contract.hpp:347-446.
+    void contract(const Level<O, E, W>& L, const O* map, O nc, Level<O, E, W>& C, DBuf<O>* skey_buf, DBuf<W>* sval_buf) {
+        auto g = L.view();
+        O n = L.n;
+        DBuf<O> cnt(nc + 1, s), moff(nc + 1, s), members(n > 0 ? n : 1, s), ucnt(nc + 1, s);
+        DBuf<E> du(nc + 1, s), hrow(nc + 1, s);
+        C.own_vw.alloc(nc, s);
+        cnt.zero(); du.zero(); C.own_vw.zero(); ucnt.zero();
+        k_contract_count<O, E, W><<<grid_persistent(n, 16), BLOCK, 0, s>>>(g, map, cnt.p, du.p, C.own_vw.p);
+        JET_LAUNCH_CHECK();
+        exclusive_scan_array<O>(cnt.p, nc + 1, moff.p, nullptr, scan, s);
+        exclusive_scan_array<E>(du.p, nc + 1, hrow.p, nullptr, scan, s);
+        k_contract_members<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, map, moff.p, cnt.p, members.p);
+        JET_LAUNCH_CHECK();
+        // scratch for unique entries, sized by the fine nnz (the bound on sum du)
+        DBuf<O> skey_own;
+        DBuf<W> sval_own;
+        O* skey;
+        W* sval;
+        if (skey_buf && skey_buf->n >= (int64_t)L.m) { skey = skey_buf->p; sval = sval_buf->p; }
+        else { skey_own.alloc(L.m > 0 ? L.m : 1, s); sval_own.alloc(L.m > 0 ? L.m : 1, s); skey = skey_own.p; sval = sval_own.p; }
+        DBuf<O> l1(nc, s), l2(nc, s), lh(nc, s);
+        O* n1 = dslot<O>(40);
+        O* n2 = dslot<O>(41);
+        O* nh = dslot<O>(42);
+        int* err = dslot<int>(43);
+        JET_CUDA(cudaMemsetAsync(n1, 0, 4 * sizeof(int64_t), s));
+        k_contract_bin<O, E><<<grid_persistent(nc, 8), BLOCK, 0, s>>>(nc, hrow.p, l1.p, n1, l2.p, n2, lh.p, nh);
+        JET_LAUNCH_CHECK();
+        k_contract_warp<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(g, map, nc, moff.p, members.p, hrow.p, skey, sval, ucnt.p);
+        JET_LAUNCH_CHECK();
+        {
+            size_t sm1 = contract_smem_bytes<O, W>(CT_S1_SLOTS), sm2 = contract_smem_bytes<O, W>(CT_S2_SLOTS);
+            JET_CUDA(cudaFuncSetAttribute(k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+            k_contract_smem<CT_S1_THREADS, CT_S1_SLOTS, O, E, W><<<device_info().sms * 8, CT_S1_THREADS, sm1, s>>>(
+                g, map, l1.p, n1, moff.p, members.p, hrow.p, skey, sval, ucnt.p);
+            JET_LAUNCH_CHECK();
+            k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W><<<device_info().sms * 2, CT_S2_THREADS, sm2, s>>>(
+                g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p);
+            JET_LAUNCH_CHECK();
+            k_contract_hub<O, E, W><<<device_info().sms, 1024, 0, s>>>(g, map, lh.p, nh, moff.p, members.p, hrow.p, skey, sval, ucnt.p, err);
+            JET_LAUNCH_CHECK();
+        }
+        // coarse row offsets and nnz
+        C.own_row.alloc(nc + 1, s);
+        E* tot = dslot<E>(44);
+        exclusive_scan<E, GetCast<O, E>>(GetCast<O, E>{ucnt.p}, nc + 1, C.own_row.p, tot, scan, s);
+        JET_CUDA(cudaMemcpyAsync(hscal, dscal.p + 40, sizeof(int64_t) * 5, cudaMemcpyDeviceToHost, s));
+        sync();
+        if (*(int*)&hscal[3]) throw JetError{JET_ERR_OVERFLOW, "contraction hash table overflow"};
+        E mc = *(E*)&hscal[4];
+        C.n = nc;
+        C.m = mc;
+        C.own_adj.alloc(mc > 0 ? mc : 1, s);
+        C.own_val.alloc(mc > 0 ? mc : 1, s);
+        k_contract_copy<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(nc, hrow.p, skey, sval, C.own_row.p,
+                                                                                        C.own_adj.p, C.own_val.p);
+        JET_LAUNCH_CHECK();
+        k_contract_copy_hub<O, E, W><<<device_info().sms, 1024, 0, s>>>(lh.p, nh, hrow.p, skey, sval, C.own_row.p, C.own_adj.p, C.own_val.p);
+        JET_LAUNCH_CHECK();
+        C.row = C.own_row.p;
+        C.adj = C.own_adj.p;
+        C.val = C.own_val.p;
+        C.vw = C.own_vw.p;
+        C.uniform = false;
+    }
+};
+
+}  // namespace jetb

@@ -1,0 +1,1021 @@
+// refine.cuh -- Jet refinement kernels (src/jet_refiner.hpp of the reference).
+//
+// Connectivity tables: vertex i owns cap(i) = min(deg(i), k) slots starting at
+// coff[i]; the first csize[i] of them form an open-addressed table part ->
+// summed edge weight (home slot p % size, linear probing; direct-mapped when
+// size == k).  Slots are {part, weight} pairs so a probe and its update touch
+// one cache line.  Table sizes follow the reference exactly: built at cap,
+// shrunk to used + max(used/4, 3) when that is smaller, grown by appends when
+// an incremental insert finds no free slot.
+//
+// Ties between equally connected destination parts go to the lowest part id
+// (the reference takes the first hash slot, which depends on slot layout).
+#pragma once
+#include "graph.cuh"
+
+namespace jetb {
+
+template <class W>
+struct Slot {
+    part_t p;
+    W v;
+};
+
+__host__ __device__ __forceinline__ part_t shrunk_size(part_t used, part_t cap) {
+    part_t q = used / 4;
+    if (q < 3) q = 3;
+    part_t s = used + q;
+    return s < cap ? s : cap;
+}
+
+template <class E>
+__host__ __device__ __forceinline__ part_t conn_cap(E deg, part_t k) { return deg > (E)k ? k : (part_t)deg; }
+
+template <class O, class E>
+struct GetConnCap {
+    const E* row;
+    part_t k;
+    __device__ __forceinline__ E operator()(int64_t i) const { return (E)conn_cap<E>(row[i + 1] - row[i], k); }
+};
+
+// Device-resident per-iteration counters and results.
+template <class O, class W>
+struct RefDev {
+    O ncand;
+    O nmoves;
+    O ncand_hub;
+    O nmoves_hub;
+    W cut1, cut2;
+    W vw_cursor;          // strong rebalance: next free position past the evictions
+    W max_vwgt;
+    part_t total_undersized;
+    int err;
+    int large;            // this iteration used update_large
+};
+// Copied to pinned host memory once per iteration.
+struct IterResult {
+    int64_t nmoves;
+    int64_t cut_change;
+    int64_t max_part;
+    int32_t err;
+    int32_t large;
+};
+
+template <class O, class E, class W>
+struct RefArgs {
+    GView<O, E, W> g;
+    part_t k;
+    const E* coff;
+    Slot<W>* slots;
+    part_t* csize;
+    part_t* dest_cache;
+    uint8_t* lock;
+    uint8_t* mark;
+    part_t* part;
+    part_t* dest;
+    W* save_gain;
+    W* pregain;
+    W* sizes;
+    O* cand;
+    O* cand_hub;
+    O* moves;
+    O* moves_hub;
+    RefDev<O, W>* dev;
+};
+
+// ---------------------------------------------------------------- table build
+// Writes a final table of `size` slots into the vertex's region from a list of
+// (part, weight) pairs held by the caller; region must be cleared first.
+template <class W>
+__device__ __forceinline__ bool table_put_private(Slot<W>* base, part_t size, part_t k, part_t p, W w) {
+    part_t po = p % size;
+    if (size < k) {
+        part_t guard = 0;
+        while (base[po].p != NULL_PART) {
+            po = (po + 1) % size;
+            if (++guard > size) return false;
+        }
+    }
+    base[po].p = p;
+    base[po].v = w;
+    return true;
+}
+
+// deg <= 32: one thread per vertex, its distinct parts gathered in a private
+// 32-entry shared-memory set (interleaved so threads hit distinct banks).
+template <class O, class E, class W>
+__global__ void __launch_bounds__(128) k_conn_thread(RefArgs<O, E, W> a, int only_marked, const int* gate) {
+    __shared__ part_t sk[32][128];
+    __shared__ W sv[32][128];
+    if (gate && !*gate) return;
+    const int t = threadIdx.x;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + t; x < a.g.n; x += (int64_t)gridDim.x * blockDim.x) {
+        O i = (O)x;
+        E rs = a.g.row[i], re = a.g.row[i + 1];
+        E deg = re - rs;
+        if (deg > THREAD_DEG) continue;
+        if (only_marked && !a.mark[i]) continue;
+        for (int s = 0; s < (int)deg; s++) sk[s][t] = NULL_PART;
+        int used = 0;
+        int sz = (int)deg;  // set capacity: at most deg distinct parts
+        bool ok = true;
+        for (E j = rs; j < re; j++) {
+            part_t p = a.part[a.g.adj[j]];
+            W w = a.g.val[j];
+            int h = p % sz;
+            int guard = 0;
+            while (sk[h][t] != NULL_PART && sk[h][t] != p && ++guard <= sz) h = h + 1 == sz ? 0 : h + 1;
+            if (guard > sz) { ok = false; break; }
+            if (sk[h][t] == NULL_PART) { sk[h][t] = p; sv[h][t] = w; used++; }
+            else sv[h][t] += w;
+        }
+        part_t cap = conn_cap<E>(deg, a.k);
+        part_t size = cap == 0 ? 0 : shrunk_size(used, cap);
+        Slot<W>* base = a.slots + a.coff[i];
+        for (int s = 0; s < cap; s++) { base[s].p = NULL_PART; base[s].v = 0; }
+        for (int s = 0; ok && s < sz; s++) {
+            part_t p = sk[s][t];
+            if (p != NULL_PART) ok = table_put_private<W>(base, size, a.k, p, sv[s][t]);
+        }
+        if (!ok) atomicOr(&a.dev->err, ERRF_OVERFLOW);
+        a.csize[i] = size;
+        if (only_marked) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
+    }
+}
+
+// Inserts p into a shared-memory table of `cap` slots (direct-mapped when
+// cap == k); returns true when this call claimed a new slot.
+// `err` receives ERRF_OVERFLOW if the probe sequence exceeds its bound (the
+// table always has room: cap >= number of distinct neighbour parts).
+template <class W>
+__device__ __forceinline__ bool smem_table_add(part_t* keys, W* vals, part_t cap, part_t k, part_t p, W w, int* err) {
+    volatile part_t* vk = keys;
+    part_t po = p % cap;
+    bool claimed = false;
+    if (cap == k) {
+        if (vk[po] == NULL_PART && atomicCAS((int*)&keys[po], NULL_PART, p) == NULL_PART) claimed = true;
+    } else {
+        int guard = 0;
+        while (true) {
+            part_t px = vk[po];
+            while (px != p && px != NULL_PART) {
+                po = po + 1 == cap ? 0 : po + 1;
+                px = vk[po];
+                if (++guard > 2 * cap) { atomicOr(err, ERRF_OVERFLOW); return false; }
+            }
+            if (px == p) break;
+            px = atomicCAS((int*)&keys[po], NULL_PART, p);
+            if (px == NULL_PART) { claimed = true; break; }
+            if (px == p) break;
+            po = po + 1 == cap ? 0 : po + 1;
+            if (++guard > 2 * cap) { atomicOr(err, ERRF_OVERFLOW); return false; }
+        }
+    }
+    atomic_add(&vals[po], w);
+    return claimed;
+}
+
+// Copies a shared-memory table (cap slots, `used` parts) to the vertex's
+// global region at its final size.  `tid`/`nt` are the cooperating threads.
+template <class W>
+__device__ __forceinline__ void smem_table_flush(const part_t* keys, const W* vals, part_t cap, part_t used, part_t k,
+                                                 Slot<W>* base, part_t* size_out, int tid, int nt, bool sync_block, int* err) {
+    part_t size = shrunk_size(used, cap);
+    if (size == cap) {
+        for (int s = tid; s < cap; s += nt) { base[s].p = keys[s]; base[s].v = vals[s]; }
+    } else {
+        for (int s = tid; s < cap; s += nt) { base[s].p = NULL_PART; base[s].v = 0; }
+        if (sync_block) __syncthreads(); else __syncwarp();
+        for (int s = tid; s < cap; s += nt) {
+            part_t p = keys[s];
+            if (p == NULL_PART) continue;
+            part_t po = p % size;
+            int guard = 0;
+            bool placed = true;
+            while (true) {
+                part_t old = atomicCAS((int*)&base[po].p, NULL_PART, p);
+                if (old == NULL_PART) break;
+                po = po + 1 == size ? 0 : po + 1;
+                if (++guard > size) { atomicOr(err, ERRF_OVERFLOW); placed = false; break; }
+            }
+            if (placed) base[po].v = vals[s];
+        }
+    }
+    if (tid == 0) *size_out = size;
+}
+
+// 32 < deg <= 4096 and k <= WARP_TABLE: one warp per vertex, table in shared memory.
+static constexpr int WARP_TABLE = 512;
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_conn_warp(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (gate && !*gate) return;
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int kw = a.k < WARP_TABLE ? a.k : WARP_TABLE;
+    part_t* keys = (part_t*)smem_raw + wid * kw;
+    W* vals = (W*)(smem_raw + (BLOCK / 32) * kw * sizeof(part_t) + ((BLOCK / 32) * kw * sizeof(part_t)) % 8) + wid * kw;
+    const int64_t warps = (int64_t)gridDim.x * (BLOCK / 32);
+    for (int64_t x = blockIdx.x * (int64_t)(BLOCK / 32) + wid; x < count; x += warps) {
+        O i = list[x];
+        if (only_marked && !a.mark[i]) continue;
+        E rs = a.g.row[i], re = a.g.row[i + 1];
+        part_t cap = conn_cap<E>(re - rs, a.k);
+        for (int s = lane; s < cap; s += 32) { keys[s] = NULL_PART; vals[s] = 0; }
+        __syncwarp();
+        int mine = 0;
+        for (E j = rs + lane; j < re; j += 32) mine += smem_table_add<W>(keys, vals, cap, a.k, a.part[a.g.adj[j]], a.g.val[j], &a.dev->err);
+        __syncwarp();
+        int used = group_sum<int>(mine, 32);
+        smem_table_flush<W>(keys, vals, cap, used, a.k, a.slots + a.coff[i], &a.csize[i], lane, 32, false, &a.dev->err);
+        if (only_marked && lane == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
+        __syncwarp();
+    }
+}
+
+// Any degree: one CTA per vertex, table of cap <= k slots in shared memory.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int s_used;
+    if (gate && !*gate) return;
+    part_t* keys = (part_t*)smem_raw;
+    W* vals = (W*)(smem_raw + ((a.k * sizeof(part_t) + 15) & ~(size_t)15));
+    for (O x = blockIdx.x; x < count; x += gridDim.x) {
+        O i = list[x];
+        if (only_marked && !a.mark[i]) continue;
+        E rs = a.g.row[i], re = a.g.row[i + 1];
+        part_t cap = conn_cap<E>(re - rs, a.k);
+        for (int s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = NULL_PART; vals[s] = 0; }
+        if (threadIdx.x == 0) s_used = 0;
+        __syncthreads();
+        int mine = 0;
+        for (E j = rs + threadIdx.x; j < re; j += blockDim.x) mine += smem_table_add<W>(keys, vals, cap, a.k, a.part[a.g.adj[j]], a.g.val[j], &a.dev->err);
+        mine = group_sum<int>(mine, 32);
+        if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&s_used, mine);
+        __syncthreads();
+        smem_table_flush<W>(keys, vals, cap, s_used, a.k, a.slots + a.coff[i], &a.csize[i], threadIdx.x, blockDim.x, true, &a.dev->err);
+        if (only_marked && threadIdx.x == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- lookups
+template <class W>
+__device__ __forceinline__ W table_lookup(const Slot<W>* base, part_t target, part_t size) {  // src/jet_refiner.hpp:891-901
+    for (part_t q = 0; q < size; q++) {
+        part_t pi = (target + q) % size;
+        part_t e = base[pi].p;
+        if (e == target) return base[pi].v;
+        if (e == NULL_PART) return 0;
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------- LP select
+// Best destination (most connected part other than the own one; ties to the
+// lowest part id) and the filter of src/jet_refiner.hpp:206-251, then the
+// candidate list of :255-266.
+template <class W>
+__device__ __forceinline__ bool lp_better(W c, part_t e, W bc, part_t be) {
+    return c > 0 && (c > bc || (c == bc && e < be));
+}
+
+template <class O, class E, class W>
+__device__ __forceinline__ void lp_finish(const RefArgs<O, E, W>& a, O i, part_t best, W b_conn, W p_conn, double filter_ratio,
+                                          bool computed) {
+    if (computed) {
+        W sg = 0;
+        if (best != NO_MOVE) {
+            if (b_conn >= p_conn || ((double)(p_conn - b_conn) < floor(filter_ratio * (double)p_conn))) sg = b_conn - p_conn;
+            else best = NO_MOVE;
+        }
+        a.save_gain[i] = sg;
+        a.dest_cache[i] = best;
+    }
+    a.dest[i] = best;
+}
+
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_lp_select_thread(RefArgs<O, E, W> a, double filter_ratio) {
+    const W GAIN_MIN = std::numeric_limits<W>::lowest();
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t rounds = ceil_div<int64_t>((int64_t)a.g.n, stride);
+    for (int64_t r = 0; r < rounds; r++) {
+        int64_t x = start + r * stride;
+        bool cand = false;
+        O i = (O)x;
+        if (x < a.g.n && a.g.row[i + 1] - a.g.row[i] <= THREAD_DEG) {
+            part_t best = a.dest_cache[i];
+            if (best != NULL_PART) {
+                lp_finish<O, E, W>(a, i, best, 0, 0, filter_ratio, false);
+            } else {
+                part_t p = a.part[i];
+                best = NO_MOVE;
+                W b_conn = 0, p_conn = 0;
+                const Slot<W>* base = a.slots + a.coff[i];
+                part_t sz = a.csize[i];
+                for (part_t s = 0; s < sz; s++) {
+                    Slot<W> sl = base[s];
+                    if (sl.p != p) { if (lp_better<W>(sl.v, sl.p, b_conn, best)) { best = sl.p; b_conn = sl.v; } }
+                    else if (sl.v > 0) p_conn = sl.v;
+                }
+                lp_finish<O, E, W>(a, i, best, b_conn, p_conn, filter_ratio, true);
+                best = a.dest[i];
+            }
+            cand = best != NO_MOVE && a.lock[i] == 0;
+            if (cand) a.pregain[i] = a.save_gain[i];
+            else { a.pregain[i] = GAIN_MIN; a.lock[i] = 0; }
+        }
+        O s = warp_append(&a.dev->ncand, cand);
+        if (cand) a.cand[s] = i;
+    }
+}
+
+// Vertices with deg > 32: one warp per vertex scans its table.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_lp_select_warp(RefArgs<O, E, W> a, const O* list, O count, double filter_ratio) {
+    const W GAIN_MIN = std::numeric_limits<W>::lowest();
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (BLOCK / 32);
+    for (int64_t x = blockIdx.x * (int64_t)(BLOCK / 32) + (threadIdx.x >> 5); x < count; x += warps) {
+        O i = list[x];
+        part_t best = a.dest_cache[i];
+        if (best != NULL_PART) {
+            if (lane == 0) lp_finish<O, E, W>(a, i, best, 0, 0, filter_ratio, false);
+        } else {
+            part_t p = a.part[i];
+            best = NO_MOVE;
+            W b_conn = 0, p_conn = 0;
+            const Slot<W>* base = a.slots + a.coff[i];
+            part_t sz = a.csize[i];
+            for (part_t s = lane; s < sz; s += 32) {
+                Slot<W> sl = base[s];
+                if (sl.p != p) { if (lp_better<W>(sl.v, sl.p, b_conn, best)) { best = sl.p; b_conn = sl.v; } }
+                else if (sl.v > 0) p_conn = sl.v;
+            }
+            for (int m = 16; m > 0; m >>= 1) {
+                W c2 = shfl_xor(b_conn, m, 32);
+                part_t e2 = shfl_xor(best, m, 32);
+                if (lp_better<W>(c2, e2, b_conn, best)) { b_conn = c2; best = e2; }
+                W pc2 = shfl_xor(p_conn, m, 32);
+                if (pc2 > p_conn) p_conn = pc2;
+            }
+            if (lane == 0) lp_finish<O, E, W>(a, i, best, b_conn, p_conn, filter_ratio, true);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            best = a.dest[i];
+            bool cand = best != NO_MOVE && a.lock[i] == 0;
+            if (cand) {
+                a.pregain[i] = a.save_gain[i];
+                O s = atomic_add(&a.dev->ncand, (O)1);
+                a.cand[s] = i;
+            } else {
+                a.pregain[i] = GAIN_MIN;
+                a.lock[i] = 0;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- afterburner
+// src/jet_refiner.hpp:275-307: a candidate keeps its move if its gain,
+// recomputed assuming every higher-priority candidate (larger pre-gain, then
+// smaller id) has already moved, is non-negative.
+template <class O, class E, class W>
+__device__ __forceinline__ W afterburn_edge(const RefArgs<O, E, W>& a, O i, W igain, part_t p, part_t best, E j) {
+    O v = a.g.adj[j];
+    W vgain = a.pregain[v];
+    W ch = 0;
+    if (vgain > igain || (vgain == igain && v < i)) {
+        W w = a.g.val[j];
+        part_t vp = a.dest[v];
+        if (vp == p) ch -= w; else if (vp == best) ch += w;
+        vp = a.part[v];
+        if (vp == p) ch += w; else if (vp == best) ch -= w;
+    }
+    return ch;
+}
+
+template <int G, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_afterburn(RefArgs<O, E, W> a) {
+    O count = a.dev->ncand;
+#define AB_BODY(x, in, lane)                                                                \
+    {                                                                                       \
+        O i = 0; E s = 0, e = 0; W igain = 0; part_t p = 0, best = 0; bool act = false;     \
+        if (in) {                                                                           \
+            i = a.cand[x]; s = a.g.row[i]; e = a.g.row[i + 1];                              \
+            act = e - s <= HUB_DEG;                                                         \
+            igain = a.pregain[i]; p = a.part[i]; best = a.dest[i];                          \
+        }                                                                                   \
+        W ch = 0;                                                                           \
+        if (act) for (E j = s + lane; j < e; j += G) ch += afterburn_edge<O, E, W>(a, i, igain, p, best, j); \
+        ch = group_sum<W>(ch, G);                                                           \
+        bool keep = act && lane == 0 && igain + ch >= 0;                                    \
+        if (keep) a.lock[i] = 1;                                                            \
+        O sl = warp_append(&a.dev->nmoves, keep);                                           \
+        if (keep) a.moves[sl] = i;                                                          \
+        if (in && lane == 0 && !act) { O hs = atomic_add(&a.dev->ncand_hub, (O)1); a.cand_hub[hs] = i; } \
+    }
+    JET_GROUP_LOOP(G, count, AB_BODY)
+#undef AB_BODY
+}
+
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_afterburn_hub(RefArgs<O, E, W> a) {
+    __shared__ W part_sum[32];
+    O count = a.dev->ncand_hub;
+    for (O x = blockIdx.x; x < count; x += gridDim.x) {
+        O i = a.cand_hub[x];
+        W igain = a.pregain[i];
+        part_t p = a.part[i], best = a.dest[i];
+        W ch = 0;
+        for (E j = a.g.row[i] + threadIdx.x; j < a.g.row[i + 1]; j += blockDim.x) ch += afterburn_edge<O, E, W>(a, i, igain, p, best, j);
+        ch = group_sum<W>(ch, 32);
+        if ((threadIdx.x & 31) == 0) part_sum[threadIdx.x >> 5] = ch;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < (int)(blockDim.x >> 5); w++) ch += part_sum[w];
+            if (igain + ch >= 0) {
+                a.lock[i] = 1;
+                O s = atomic_add(&a.dev->nmoves, (O)1);
+                a.moves[s] = i;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- gain buckets
+// src/jet_refiner.hpp:326-356 with C++ semantics kept: the float gain is
+// scaled by the double literal 1.5 in double and rounded back to float.
+template <class W>
+__host__ __device__ __forceinline__ int gain_bucket(W gx, W vwgt) {
+    float gain = (float)gx / (float)vwgt;
+    int t;
+    if (gain > 0.0) t = 0;
+    else if (gain == 0.0) t = 1;
+    else {
+        t = MID_BUCKET;
+        gain = fabsf(gain);
+        if (gain < 1.0) {
+            while (gain < 1.0) { gain = (float)((double)gain * 1.5); t--; }
+            if (t < 2) t = 2;
+        } else {
+            while (gain > 1.0) { gain = (float)((double)gain / 1.5); t++; }
+            if (t > MAX_BUCKETS) t = MAX_BUCKETS - 1;
+        }
+    }
+    return t;
+}
+
+// ---------------------------------------------------------------- rebalance
+template <class O, class W>
+struct RebArgs {
+    W size_max;
+    W opt;
+    W max_dest;
+    O sections;
+    O t_minibuckets;
+    O width;          // MAX_BUCKETS * sections
+    W* buckets;       // t_minibuckets + 1 + width entries
+    O* bid;
+    W* score;
+    part_t* undersized;
+    W* evict_adjust;  // k
+    W* evict_start;   // k + 1
+};
+
+// Undersized parts in index order (src/jet_refiner.hpp:584-598).
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_weak_prep(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    __shared__ int sw[32];
+    int carry = 0;
+    for (int base = 0; base < a.k; base += 1024) {
+        int p = base + threadIdx.x;
+        int f = (p < a.k && a.sizes[p] < rb.max_dest) ? 1 : 0;
+        int tot;
+        int ex = block_exclusive_scan<int>(f, sw, tot);
+        if (f) rb.undersized[carry + ex] = p;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) a.dev->total_undersized = carry;
+}
+
+// Destination choice and bucket score (src/jet_refiner.hpp:599-645), one
+// thread per vertex (tables of vertices with deg > 32 are scanned by a warp).
+template <class O, class E, class W>
+__device__ __forceinline__ void weak_score(const RefArgs<O, E, W>& a, const RebArgs<O, W>& rb, O i, part_t p, part_t best,
+                                           W gain, W p_gain, bool eligible) {
+    part_t dest = p;
+    W sg = 0;
+    if (eligible) {
+        if (gain > 0) { dest = best; sg = gain - p_gain; }
+        else {
+            part_t tu = a.dev->total_undersized;
+            if (tu > 0) { dest = rb.undersized[(int64_t)i % tu]; sg = -p_gain; }
+        }
+    }
+    a.dest[i] = dest;
+    if (dest != p) {
+        int gt = gain_bucket<W>(sg, a.g.vw[i]);
+        O gid = (MAX_BUCKETS * (O)p + gt) * rb.sections + (O)(i % rb.sections);
+        rb.bid[i] = gid;
+        rb.score[i] = atomic_add(&rb.buckets[gid], a.g.vw[i]);
+    } else {
+        rb.bid[i] = -1;
+    }
+}
+
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_weak_select_thread(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < a.g.n; x += (int64_t)gridDim.x * blockDim.x) {
+        O i = (O)x;
+        if (a.g.row[i + 1] - a.g.row[i] > THREAD_DEG) continue;
+        part_t p = a.part[i];
+        W sp = a.sizes[p];
+        bool elig = sp > rb.size_max && (double)a.g.vw[i] < 1.5 * (double)(sp - rb.opt);
+        W gain = 0, p_gain = 0;
+        part_t best = p;
+        if (elig) {
+            const Slot<W>* base = a.slots + a.coff[i];
+            part_t sz = a.csize[i];
+            for (part_t s = 0; s < sz; s++) {
+                Slot<W> sl = base[s];
+                if (sl.p > NULL_PART && a.sizes[sl.p] < rb.max_dest) {
+                    if (sl.v > gain || (sl.v == gain && sl.v > 0 && sl.p < best)) { best = sl.p; gain = sl.v; }
+                }
+                if (sl.p == p) p_gain = sl.v;
+            }
+        }
+        weak_score<O, E, W>(a, rb, i, p, best, gain, p_gain, elig);
+    }
+}
+
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_weak_select_warp(RefArgs<O, E, W> a, RebArgs<O, W> rb, const O* list, O count) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (BLOCK / 32);
+    for (int64_t x = blockIdx.x * (int64_t)(BLOCK / 32) + (threadIdx.x >> 5); x < count; x += warps) {
+        O i = list[x];
+        part_t p = a.part[i];
+        W sp = a.sizes[p];
+        bool elig = sp > rb.size_max && (double)a.g.vw[i] < 1.5 * (double)(sp - rb.opt);
+        W gain = 0, p_gain = 0;
+        part_t best = p;
+        if (elig) {
+            const Slot<W>* base = a.slots + a.coff[i];
+            part_t sz = a.csize[i];
+            for (part_t s = lane; s < sz; s += 32) {
+                Slot<W> sl = base[s];
+                if (sl.p > NULL_PART && a.sizes[sl.p] < rb.max_dest) {
+                    if (sl.v > gain || (sl.v == gain && sl.v > 0 && sl.p < best)) { best = sl.p; gain = sl.v; }
+                }
+                if (sl.p == p) p_gain = sl.v;
+            }
+            for (int m = 16; m > 0; m >>= 1) {
+                W g2 = shfl_xor(gain, m, 32);
+                part_t b2 = shfl_xor(best, m, 32);
+                if (g2 > gain || (g2 == gain && g2 > 0 && b2 < best)) { gain = g2; best = b2; }
+                W pg2 = shfl_xor(p_gain, m, 32);
+                if (pg2 != 0) p_gain = pg2;
+            }
+        }
+        if (lane == 0) weak_score<O, E, W>(a, rb, i, p, best, gain, p_gain, elig);
+    }
+}
+
+// max_vwgt: largest room left in a part below max_dest (src/jet_refiner.hpp:442-451).
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_strong_prep(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    __shared__ W sm[32];
+    __shared__ int sany[32];
+    W best = std::numeric_limits<W>::lowest();
+    int any = 0;
+    for (int p = threadIdx.x; p < a.k; p += blockDim.x) {
+        W s = a.sizes[p];
+        if (s < rb.max_dest) { W cap = rb.max_dest - s; if (!any || cap > best) best = cap; any = 1; }
+    }
+    for (int m = 16; m > 0; m >>= 1) {
+        W b2 = shfl_xor(best, m, 32);
+        int a2 = shfl_xor(any, m, 32);
+        if (a2 && (!any || b2 > best)) best = b2;
+        any |= a2;
+    }
+    if ((threadIdx.x & 31) == 0) { sm[threadIdx.x >> 5] = best; sany[threadIdx.x >> 5] = any; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++)
+            if (sany[w] && (!any || sm[w] > best)) { best = sm[w]; any = 1; }
+        a.dev->max_vwgt = any ? best : std::numeric_limits<W>::lowest();
+        a.dev->total_undersized = any;
+    }
+}
+
+// Eviction score: average loss to adjacent non-full parts (unsigned
+// division, src/jet_refiner.hpp:452-480).
+template <class O, class E, class W>
+__device__ __forceinline__ void strong_score(const RefArgs<O, E, W>& a, const RebArgs<O, W>& rb, O i, part_t p, uint64_t tg,
+                                             uint64_t tk, W p_gain) {
+    if (tk == 0) tk = 1;
+    W gain = (W)((tg / tk) - (uint64_t)p_gain);
+    W w = a.g.vw[i];
+    W lim = a.sizes[p] - rb.size_max;
+    int gt = gain_bucket<W>(gain, w < lim ? w : lim);
+    if (gt < MAX_BUCKETS) {
+        O gid = (MAX_BUCKETS * (O)p + gt) * rb.sections + (O)(i % rb.sections) + 1;
+        rb.bid[i] = gid;
+        rb.score[i] = atomic_add(&rb.buckets[gid], w);
+    }
+}
+
+template <class O, class E, class W>
+__device__ __forceinline__ bool strong_eligible(const RefArgs<O, E, W>& a, const RebArgs<O, W>& rb, O i, part_t p) {
+    W sp = a.sizes[p];
+    W w = a.g.vw[i];
+    if (!a.dev->total_undersized) return false;  // no part below max_dest
+    W mv = a.dev->max_vwgt;
+    return sp > rb.size_max && w <= 2 * mv && w < 2 * (sp - rb.opt);
+}
+
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_strong_score_thread(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < a.g.n; x += (int64_t)gridDim.x * blockDim.x) {
+        O i = (O)x;
+        if (a.g.row[i + 1] - a.g.row[i] > THREAD_DEG) continue;
+        part_t p = a.part[i];
+        rb.bid[i] = -1;
+        if (!strong_eligible<O, E, W>(a, rb, i, p)) continue;
+        uint64_t tk = 0, tg = 0;
+        W p_gain = 0;
+        const Slot<W>* base = a.slots + a.coff[i];
+        part_t sz = a.csize[i];
+        for (part_t s = 0; s < sz; s++) {
+            Slot<W> sl = base[s];
+            if (sl.p == p) p_gain = sl.v;
+            else if (sl.p > NULL_PART && a.sizes[sl.p] < rb.max_dest) { tg += (uint64_t)sl.v; tk += 1; }
+        }
+        strong_score<O, E, W>(a, rb, i, p, tg, tk, p_gain);
+    }
+}
+
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_strong_score_warp(RefArgs<O, E, W> a, RebArgs<O, W> rb, const O* list, O count) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (BLOCK / 32);
+    for (int64_t x = blockIdx.x * (int64_t)(BLOCK / 32) + (threadIdx.x >> 5); x < count; x += warps) {
+        O i = list[x];
+        part_t p = a.part[i];
+        if (lane == 0) rb.bid[i] = -1;
+        if (!strong_eligible<O, E, W>(a, rb, i, p)) continue;
+        uint64_t tk = 0, tg = 0;
+        W p_gain = 0;
+        const Slot<W>* base = a.slots + a.coff[i];
+        part_t sz = a.csize[i];
+        for (part_t s = lane; s < sz; s += 32) {
+            Slot<W> sl = base[s];
+            if (sl.p == p) p_gain = sl.v;
+            else if (sl.p > NULL_PART && a.sizes[sl.p] < rb.max_dest) { tg += (uint64_t)sl.v; tk += 1; }
+        }
+        tg = group_sum<uint64_t>(tg, 32);
+        tk = group_sum<uint64_t>(tk, 32);
+        p_gain = group_sum<W>(p_gain, 32);  // own part appears in at most one slot
+        if (lane == 0) strong_score<O, E, W>(a, rb, i, p, tg, tk, p_gain);
+    }
+}
+
+// get_evictions (src/jet_refiner.hpp:392-409): `buckets` already holds the
+// exclusive offsets.
+template <bool ADJUST, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_evict(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t rounds = ceil_div<int64_t>((int64_t)a.g.n, stride);
+    for (int64_t r = 0; r < rounds; r++) {
+        int64_t x = start + r * stride;
+        bool take = false;
+        O i = (O)x;
+        if (x < a.g.n) {
+            O b = rb.bid[i];
+            if (b != -1) {
+                part_t p = a.part[i];
+                O begin = (O)p * rb.width;
+                W score = rb.score[i] + rb.buckets[b] - rb.buckets[begin];
+                W limit = a.sizes[p] - rb.size_max;
+                if (score < limit) {
+                    take = true;
+                    if (ADJUST && score + a.g.vw[i] >= limit) rb.evict_adjust[p] = score + a.g.vw[i];
+                }
+            }
+        }
+        O s = warp_append(&a.dev->nmoves, take);
+        if (take) a.moves[s] = i;
+    }
+}
+
+// "cookie cutter" (src/jet_refiner.hpp:491-518): prefix positions of the
+// evicted weight per part and of the free room per undersized part.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_cookie(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    __shared__ W sw[32];
+    W carry = 0;
+    for (int base = 0; base < a.k; base += 1024) {
+        int p = base + threadIdx.x;
+        W add = 0;
+        O begin = (O)p * rb.width;
+        if (p < a.k) {
+            add = rb.evict_adjust[p];
+            if (add == 0) add = rb.buckets[begin + rb.width] - rb.buckets[begin];
+        }
+        W tot;
+        W ex = block_exclusive_scan<W>(add, sw, tot);
+        if (p < a.k) rb.evict_adjust[p] = rb.buckets[begin] - (carry + ex);
+        carry += tot;
+    }
+    if (threadIdx.x == 0) a.dev->vw_cursor = carry;
+    W carry2 = 0;
+    for (int base = 0; base < a.k; base += 1024) {
+        int p = base + threadIdx.x;
+        W add = 0;
+        if (p < a.k && rb.max_dest > a.sizes[p]) add = rb.max_dest - a.sizes[p];
+        W tot;
+        W ex = block_exclusive_scan<W>(add, sw, tot);
+        if (p < a.k) rb.evict_start[p + 1] = carry2 + ex + add;
+        carry2 += tot;
+    }
+    if (threadIdx.x == 0) rb.evict_start[0] = 0;
+}
+
+// Adjust scores and pick destinations by chunk, re-drawing a position past
+// the end when less than half the vertex fits (src/jet_refiner.hpp:519-544).
+template <class O, class E, class W>
+__global__ void k_strong_dest(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    O count = a.dev->nmoves;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < count; x += (int64_t)gridDim.x * blockDim.x) {
+        O v = a.moves[x];
+        part_t pv = a.part[v];
+        W sc = rb.score[v] + rb.buckets[rb.bid[v]] - rb.evict_adjust[pv];
+        W w = a.g.vw[v];
+        int p = 0;
+        part_t dest = pv;
+        // re-drawn positions only grow, so p never falls below 0; the guard
+        // bounds the walk regardless
+        int guard = 0;
+        while (p < a.k) {
+            while (p <= a.k && rb.evict_start[p] <= sc) p++;
+            p--;
+            if (p < 0 || ++guard > 4 * a.k + 64) { atomicOr(&a.dev->err, ERRF_SPIN); dest = pv; break; }
+            if (p < a.k && w / 2 <= rb.evict_start[p + 1] - sc) { dest = p; break; }
+            else if (p < a.k) sc = atomic_add(&a.dev->vw_cursor, w);
+        }
+        rb.score[v] = sc;
+        a.dest[v] = dest;
+    }
+}
+
+// ---------------------------------------------------------------- moves
+// perform_moves part 1 (src/jet_refiner.hpp:910-931): cut change from the old
+// tables, apply the moves, part-size deltas through a shared histogram.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_apply_moves(RefArgs<O, E, W> a, int hist) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    W* hs = (W*)smem_raw;
+    if (hist) {
+        for (int p = threadIdx.x; p < a.k; p += blockDim.x) hs[p] = 0;
+        __syncthreads();
+    }
+    O count = a.dev->nmoves;
+    W c1 = 0;
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < count; x += stride) {
+        O i = a.moves[x];
+        part_t p = a.part[i], b = a.dest[i];
+        const Slot<W>* base = a.slots + a.coff[i];
+        part_t sz = a.csize[i];
+        c1 += table_lookup<W>(base, b, sz) - table_lookup<W>(base, p, sz);
+        a.dest_cache[i] = NULL_PART;
+        W w = a.g.vw[i];
+        if (hist) { atomic_add(&hs[p], -w); atomic_add(&hs[b], w); }
+        else { atomic_add(&a.sizes[p], -w); atomic_add(&a.sizes[b], w); }
+        a.part[i] = b;
+        a.dest[i] = p;
+        if (a.g.row[i + 1] - a.g.row[i] > HUB_DEG) { O s = atomic_add(&a.dev->nmoves_hub, (O)1); a.moves_hub[s] = i; }
+    }
+    c1 = group_sum<W>(c1, 32);
+    if ((threadIdx.x & 31) == 0 && c1) atomic_add(&a.dev->cut1, c1);
+    if (hist) {
+        __syncthreads();
+        for (int p = threadIdx.x; p < a.k; p += blockDim.x) if (hs[p]) atomic_add(&a.sizes[p], hs[p]);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.dev->large = count > (O)(a.g.n / 10);
+}
+
+// update_small subtract (src/jet_refiner.hpp:786-808).
+template <class O, class E, class W>
+__device__ __forceinline__ void conn_sub(const RefArgs<O, E, W>& a, O v, part_t p, W w) {
+    Slot<W>* base = a.slots + a.coff[v];
+    part_t vsize = a.csize[v];
+    part_t po = p % vsize;
+    part_t guard = 0;
+    while (ld_cg(&base[po].p) != p) {
+        po = po + 1 == vsize ? 0 : po + 1;
+        if (++guard > vsize) { atomicOr(&a.dev->err, ERRF_PROBE); return; }
+    }
+    W x = atomic_add(&base[po].v, -w);
+    if (vsize < a.k && x == w) st_v(&base[po].p, HASH_RECLAIM);
+}
+
+// update_small add (src/jet_refiner.hpp:811-887).
+template <class O, class E, class W>
+__device__ __forceinline__ void conn_add(const RefArgs<O, E, W>& a, O v, part_t best, W w) {
+    a.dest_cache[v] = NULL_PART;
+    E vs = a.coff[v];
+    Slot<W>* base = a.slots + vs;
+    part_t vsize = ld_cg(&a.csize[v]);
+    part_t po = best % vsize;
+    bool success = false;
+    for (part_t q = 0; q < vsize; q++) {
+        part_t pi = (best + q) % vsize;
+        part_t e = ld_cg(&base[pi].p);
+        if (e == best) { success = true; po = pi; break; }
+        else if (e == NULL_PART) break;
+    }
+    part_t count = 0;
+    while (!success && count < vsize) {
+        part_t px = ld_cg(&base[po].p);
+        while (px != best && px > NULL_PART && count++ < vsize) {
+            po = (po + 1) % vsize;
+            px = ld_cg(&base[po].p);
+        }
+        if (px == best) success = true;
+        else if (px <= NULL_PART) {
+            part_t old = atomicCAS((int*)&base[po].p, px, best);
+            if (old == best || old <= NULL_PART) success = true;
+            else { po = (po + 1) % vsize; count++; }
+        }
+    }
+    if (!success) {
+        // no free slot: append past the table's end (capacity min(deg,k) always suffices)
+        part_t cap = (part_t)(a.coff[v + 1] - vs);
+        po = vsize;
+        while (!success) {
+            if (po >= cap) { atomicOr(&a.dev->err, ERRF_OVERFLOW); return; }
+            part_t px = ld_cg(&base[po].p);
+            while (px != best && px > NULL_PART) {
+                if (++po >= cap) { atomicOr(&a.dev->err, ERRF_OVERFLOW); return; }
+                px = ld_cg(&base[po].p);
+            }
+            if (px == best) success = true;
+            else {
+                part_t py = atomicCAS((int*)&base[po].p, px, best);
+                if (py == px) { py = best; atomicAdd((int*)&a.csize[v], 1); }
+                if (py == best) success = true;
+                else po++;
+            }
+        }
+    }
+    atomic_add(&base[po].v, w);
+}
+
+template <int G, bool ADD, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_update_small(RefArgs<O, E, W> a) {
+    if (a.dev->large) return;
+    O count = a.dev->nmoves;
+#define UPD_BODY(x, in, lane)                                                               \
+    {                                                                                       \
+        if (in) {                                                                           \
+            O i = a.moves[x];                                                               \
+            E s = a.g.row[i], e = a.g.row[i + 1];                                           \
+            if (e - s <= HUB_DEG) {                                                         \
+                part_t pp = ADD ? a.part[i] : a.dest[i];                                    \
+                for (E j = s + lane; j < e; j += G) {                                       \
+                    if (ADD) conn_add<O, E, W>(a, a.g.adj[j], pp, a.g.val[j]);              \
+                    else conn_sub<O, E, W>(a, a.g.adj[j], pp, a.g.val[j]);                  \
+                }                                                                           \
+            }                                                                               \
+        }                                                                                   \
+    }
+    JET_GROUP_LOOP(G, count, UPD_BODY)
+#undef UPD_BODY
+}
+
+template <bool ADD, class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_update_small_hub(RefArgs<O, E, W> a) {
+    if (a.dev->large) return;
+    O count = a.dev->nmoves_hub;
+    for (O x = blockIdx.x; x < count; x += gridDim.x) {
+        O i = a.moves_hub[x];
+        part_t pp = ADD ? a.part[i] : a.dest[i];
+        for (E j = a.g.row[i] + threadIdx.x; j < a.g.row[i + 1]; j += blockDim.x) {
+            if (ADD) conn_add<O, E, W>(a, a.g.adj[j], pp, a.g.val[j]);
+            else conn_sub<O, E, W>(a, a.g.adj[j], pp, a.g.val[j]);
+        }
+    }
+}
+
+// update_large (src/jet_refiner.hpp:743-777): mark every neighbour of a
+// moved vertex; the marked rows are rebuilt by the table builders.
+template <int G, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_mark_neighbors(RefArgs<O, E, W> a) {
+    if (!a.dev->large) return;
+    O count = a.dev->nmoves;
+#define MARK_BODY(x, in, lane)                                                              \
+    {                                                                                       \
+        if (in) {                                                                           \
+            O i = a.moves[x];                                                               \
+            for (E j = a.g.row[i] + lane; j < a.g.row[i + 1]; j += G) {                     \
+                O v = a.g.adj[j];                                                           \
+                if (!a.mark[v]) a.mark[v] = 1;                                              \
+            }                                                                               \
+        }                                                                                   \
+    }
+    JET_GROUP_LOOP(G, count, MARK_BODY)
+#undef MARK_BODY
+}
+
+// perform_moves part 2 (src/jet_refiner.hpp:937-946): cut change from the
+// updated tables.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_cut_after(RefArgs<O, E, W> a) {
+    O count = a.dev->nmoves;
+    W c2 = 0;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < count; x += (int64_t)gridDim.x * blockDim.x) {
+        O i = a.moves[x];
+        const Slot<W>* base = a.slots + a.coff[i];
+        part_t sz = a.csize[i];
+        c2 += table_lookup<W>(base, a.part[i], sz) - table_lookup<W>(base, a.dest[i], sz);
+    }
+    c2 = group_sum<W>(c2, 32);
+    if ((threadIdx.x & 31) == 0 && c2) atomic_add(&a.dev->cut2, c2);
+}
+
+// Largest part, results to the host mirror, counters reset.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_finalize(RefArgs<O, E, W> a, IterResult* out) {
+    __shared__ W sm[32];
+    W mx = std::numeric_limits<W>::lowest();
+    for (int p = threadIdx.x; p < a.k; p += blockDim.x) { W s = a.sizes[p]; if (s > mx) mx = s; }
+    for (int m = 16; m > 0; m >>= 1) { W y = shfl_xor(mx, m, 32); if (y > mx) mx = y; }
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) if (sm[w] > mx) mx = sm[w];
+        RefDev<O, W>* d = a.dev;
+        out->nmoves = (int64_t)d->nmoves;
+        out->cut_change = (int64_t)(d->cut1 + d->cut2);
+        out->max_part = (int64_t)mx;
+        out->err = d->err;
+        out->large = d->large;
+        d->ncand = 0; d->nmoves = 0; d->ncand_hub = 0; d->nmoves_hub = 0;
+        d->cut1 = 0; d->cut2 = 0; d->large = 0;
+    }
+}
+
+// ---------------------------------------------------------------- statistics
+// Cut counted from both endpoints (src/part_stat.hpp:77-108).
+template <int G, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_total_cut(GView<O, E, W> g, const part_t* part, W* out) {
+    W acc = 0;
+#define CUT_BODY(x, in, lane)                                                               \
+    {                                                                                       \
+        if (in) {                                                                           \
+            O i = (O)x; part_t pi = part[i];                                                \
+            for (E j = g.row[i] + lane; j < g.row[i + 1]; j += G) if (part[g.adj[j]] != pi) acc += g.val[j]; \
+        }                                                                                   \
+    }
+    JET_GROUP_LOOP(G, g.n, CUT_BODY)
+#undef CUT_BODY
+    acc = group_sum<W>(acc, 32);
+    if ((threadIdx.x & 31) == 0 && acc) atomic_add(out, acc);
+}
+
+template <class O, class W>
+__global__ void __launch_bounds__(BLOCK) k_part_sizes(O n, const W* vw, const part_t* part, part_t k, W* sizes, int hist) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    W* hs = (W*)smem_raw;
+    if (hist) { for (int p = threadIdx.x; p < k; p += blockDim.x) hs[p] = 0; __syncthreads(); }
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (hist) atomic_add(&hs[part[i]], vw[i]);
+        else atomic_add(&sizes[part[i]], vw[i]);
+    }
+    if (hist) {
+        __syncthreads();
+        for (int p = threadIdx.x; p < k; p += blockDim.x) if (hs[p]) atomic_add(&sizes[p], hs[p]);
+    }
+}
+
+// Projection to the finer level (src/uncoarsen.hpp:82-86).
+template <class O>
+__global__ void k_project(O n_fine, const O* map, const part_t* coarse, part_t* fine) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n_fine; i += (int64_t)gridDim.x * blockDim.x)
+        fine[i] = coarse[map[i]];
+}
+
+// Part ids out of range are rejected before refinement starts.
+static __global__ void k_check_parts(int64_t n, const part_t* part, part_t k, int* err) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        if (part[i] < 0 || part[i] >= k) atomicOr(err, 8);
+}
+
+}  // namespace jetb

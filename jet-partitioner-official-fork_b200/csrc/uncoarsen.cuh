@@ -1,0 +1,534 @@
+// uncoarsen.cuh -- Jet refinement driver (src/jet_refiner.hpp:1050-1142),
+// the uncoarsening loop (src/uncoarsen.hpp:88-158) and the whole partition
+// (src/partitioner.hpp:61-125).
+#pragma once
+#include "partitioner.cuh"
+
+namespace jetb {
+
+template <class O, class E, class W>
+struct Refiner {
+    Engine<O, E, W>& e;
+    cudaStream_t s;
+    part_t k;
+    O n_max;
+    int64_t slots_cap;
+    DBuf<E> coff;
+    DBuf<Slot<W>> slots;
+    DBuf<part_t> csize, dest_cache, part_work, dest, undersized;
+    DBuf<uint8_t> lock, mark;
+    DBuf<W> save_gain, pregain, score, sizes_curr, sizes_best, evict_adjust, evict_start, buckets;
+    DBuf<O> cand, cand_hub, moves, moves_hub, bid;
+    DBuf<RefDev<O, W>> dev;
+    int64_t bucket_cap = 0;
+    bool verbose = false;
+
+    struct HostState {
+        W cut = 0;
+        W total_imb = 0;
+        W total_size = 0;
+        bool init = false;
+    };
+    HostState best, curr;
+    int64_t total_iters = 0;
+
+    Refiner(Engine<O, E, W>& eng, O nmax, int64_t mmax, part_t kk) : e(eng), s(eng.s), k(kk), n_max(nmax) {
+        int64_t n1 = nmax > 0 ? nmax : 1;
+        coff.alloc(n1 + 1, s);
+        slots_cap = mmax > 0 ? mmax : 1;
+        slots.alloc(slots_cap, s);
+        csize.alloc(n1, s); dest_cache.alloc(n1, s); part_work.alloc(n1, s); dest.alloc(n1, s);
+        lock.alloc(n1, s); mark.alloc(n1, s); mark.zero();
+        save_gain.alloc(n1, s); pregain.alloc(n1, s); score.alloc(n1, s);
+        cand.alloc(n1, s); cand_hub.alloc(n1, s); moves.alloc(n1, s); moves_hub.alloc(n1, s); bid.alloc(n1, s);
+        sizes_curr.alloc(k, s); sizes_best.alloc(k, s); undersized.alloc(k, s); evict_adjust.alloc(k, s);
+        evict_start.alloc(k + 1, s);
+        O sections, tmb;
+        sections_for(nmax, sections, tmb);
+        bucket_cap = (int64_t)tmb + 1 + (int64_t)MAX_BUCKETS * sections;
+        buckets.alloc(bucket_cap, s);
+        dev.alloc(1, s);
+        dev.zero();
+    }
+
+    // src/jet_refiner.hpp:425-430 and :559-564
+    void sections_for(O n, O& sections, O& t_minibuckets) const {
+        sections = MAX_SECTIONS;
+        O section_size = (n + sections * k) / (sections * k);
+        if (section_size < 4096) {
+            section_size = 4096;
+            sections = (n + section_size * k) / (section_size * k);
+        }
+        t_minibuckets = MAX_BUCKETS * k * sections;
+    }
+
+    RefArgs<O, E, W> args(const Level<O, E, W>& L) {
+        RefArgs<O, E, W> a;
+        a.g = L.view(); a.k = k; a.coff = coff.p; a.slots = slots.p; a.csize = csize.p; a.dest_cache = dest_cache.p;
+        a.lock = lock.p; a.mark = mark.p; a.part = part_work.p; a.dest = dest.p; a.save_gain = save_gain.p;
+        a.pregain = pregain.p; a.sizes = sizes_curr.p; a.cand = cand.p; a.cand_hub = cand_hub.p; a.moves = moves.p;
+        a.moves_hub = moves_hub.p; a.dev = dev.p;
+        return a;
+    }
+
+    size_t warp_smem() const {
+        int kw = k < WARP_TABLE ? k : WARP_TABLE;
+        return (size_t)(BLOCK / 32) * kw * (sizeof(part_t) + sizeof(W)) + 16;
+    }
+    size_t cta_smem() const { return (((size_t)k * sizeof(part_t) + 15) & ~(size_t)15) + (size_t)k * sizeof(W); }
+
+    bool attrs_done = false;
+    void set_attrs() {
+        if (attrs_done) return;
+        JET_CUDA(cudaFuncSetAttribute(k_conn_warp<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp_smem_max()));
+        JET_CUDA(cudaFuncSetAttribute(k_conn_cta<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      device_info().max_smem_optin - 1024));
+        attrs_done = true;
+    }
+    static size_t warp_smem_max() { return (size_t)(BLOCK / 32) * WARP_TABLE * (sizeof(part_t) + sizeof(W)) + 16; }
+
+    // Builds (or, with only_marked, rebuilds the marked rows of) every table.
+    void build_tables(const Level<O, E, W>& L, int only_marked, const int* gate) {
+        set_attrs();
+        auto a = args(L);
+        if (cta_smem() > (size_t)device_info().max_smem_optin - 1024)
+            throw JetError{JET_ERR_INVALID, "num_parts too large for the shared-memory connectivity tables"};
+        k_conn_thread<O, E, W><<<grid_persistent(L.n, 16), 128, 0, s>>>(a, only_marked, gate);
+        JET_LAUNCH_CHECK();
+        if (L.n_warp > 0) {
+            if (k <= WARP_TABLE) {
+                k_conn_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, warp_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate);
+            } else {
+                k_conn_cta<O, E, W><<<grid_for(L.n_warp, 1) < 4096 ? grid_for(L.n_warp, 1) : 4096, 256, cta_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate);
+            }
+            JET_LAUNCH_CHECK();
+        }
+        if (L.n_hub > 0) {
+            k_conn_cta<O, E, W><<<grid_for(L.n_hub, 1) < 4096 ? grid_for(L.n_hub, 1) : 4096, 1024, cta_smem(), s>>>(a, L.hub_list.p, L.n_hub, only_marked, gate);
+            JET_LAUNCH_CHECK();
+        }
+    }
+
+    // init_conn_data, src/jet_refiner.hpp:958-1048.  Returns sum of capacities.
+    int64_t init_conn(const Level<O, E, W>& L) {
+        exclusive_scan<E, GetConnCap<O, E>>(GetConnCap<O, E>{L.row, k}, L.n, coff.p, coff.p + L.n, e.scan, s);
+        int h = prof_begin(s);
+        build_tables(L, 0, nullptr);
+        E C = 0;
+        JET_CUDA(cudaMemcpyAsync(&e.hscal[0], coff.p + L.n, sizeof(E), cudaMemcpyDeviceToHost, s));
+        e.sync();
+        C = *(E*)&e.hscal[0];
+        prof_end(h, PK_CONN_BUILD,
+                 (double)L.n * (3 * sizeof(E) + 4) + (double)L.m * (sizeof(O) + sizeof(W) + 4) + (double)C * sizeof(Slot<W>), s);
+        fill<part_t>(dest_cache.p, L.n, NULL_PART, s);
+        JET_CUDA(cudaMemsetAsync(lock.p, 0, L.n, s));
+        return (int64_t)C;
+    }
+
+    void lp(const Level<O, E, W>& L, double filter_ratio) {
+        auto a = args(L);
+        int h = prof_begin(s);
+        k_lp_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, filter_ratio);
+        JET_LAUNCH_CHECK();
+        if (L.n_warp > 0) k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, L.warp_list.p, L.n_warp, filter_ratio);
+        if (L.n_hub > 0) k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, L.hub_list.p, L.n_hub, filter_ratio);
+        JET_LAUNCH_CHECK();
+        prof_end(h, PK_LP_SELECT, 0, s);
+        h = prof_begin(s);
+        unsigned grid = grid_persistent((int64_t)L.n * L.group, 16);
+        switch (L.group) {
+            case 4: k_afterburn<4, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 8: k_afterburn<8, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 16: k_afterburn<16, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            default: k_afterburn<32, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+        }
+        JET_LAUNCH_CHECK();
+        if (L.n_hub > 0) {
+            k_afterburn_hub<O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a);
+            JET_LAUNCH_CHECK();
+        }
+        prof_end(h, PK_AFTERBURN, 0, s);
+    }
+
+    RebArgs<O, W> reb_args(const Level<O, E, W>& L, W max_dest, W opt, W size_max) {
+        RebArgs<O, W> rb;
+        O sections, tmb;
+        sections_for(L.n, sections, tmb);
+        rb.size_max = size_max; rb.opt = opt; rb.max_dest = max_dest; rb.sections = sections; rb.t_minibuckets = tmb;
+        rb.width = MAX_BUCKETS * sections; rb.buckets = buckets.p; rb.bid = bid.p; rb.score = score.p;
+        rb.undersized = undersized.p; rb.evict_adjust = evict_adjust.p; rb.evict_start = evict_start.p;
+        if ((int64_t)tmb + 1 + rb.width > bucket_cap) throw JetError{JET_ERR_INVALID, "bucket array too small"};
+        JET_CUDA(cudaMemsetAsync(buckets.p, 0, sizeof(W) * ((size_t)tmb + 1 + rb.width), s));
+        return rb;
+    }
+
+    // rebalance_weak, src/jet_refiner.hpp:551-645.
+    void weak(const Level<O, E, W>& L, W opt, W size_max) {
+        auto a = args(L);
+        W max_dest = (W)((double)size_max * 0.99);
+        if (max_dest < size_max - 100) max_dest = size_max - 100;
+        auto rb = reb_args(L, max_dest, opt, size_max);
+        k_weak_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb);
+        k_weak_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb);
+        if (L.n_warp > 0) k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp);
+        if (L.n_hub > 0) k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub);
+        JET_LAUNCH_CHECK();
+        exclusive_scan_array<W>(buckets.p, (int64_t)rb.t_minibuckets + 1, buckets.p, nullptr, e.scan, s);
+        k_evict<false, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb);
+        JET_LAUNCH_CHECK();
+    }
+
+    // rebalance_strong, src/jet_refiner.hpp:417-546.
+    void strong(const Level<O, E, W>& L, W opt, W size_max) {
+        auto a = args(L);
+        W md = (W)((double)size_max * 0.99);
+        W max_dest = opt + 1 > md ? opt + 1 : md;
+        auto rb = reb_args(L, max_dest, opt, size_max);
+        k_strong_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb);
+        k_strong_score_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb);
+        if (L.n_warp > 0) k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp);
+        if (L.n_hub > 0) k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub);
+        JET_LAUNCH_CHECK();
+        exclusive_scan_array<W>(buckets.p, (int64_t)rb.t_minibuckets + 1, buckets.p, nullptr, e.scan, s);
+        JET_CUDA(cudaMemsetAsync(evict_adjust.p, 0, sizeof(W) * k, s));
+        k_evict<true, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb);
+        k_cookie<O, E, W><<<1, 1024, 0, s>>>(a, rb);
+        k_strong_dest<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(a, rb);
+        JET_LAUNCH_CHECK();
+    }
+
+    // perform_moves, src/jet_refiner.hpp:905-955.  One host sync.
+    IterResult perform_moves(const Level<O, E, W>& L) {
+        auto a = args(L);
+        int hist = (size_t)k * sizeof(W) <= 32 * 1024;
+        k_apply_moves<O, E, W><<<grid_persistent(L.n, 8), BLOCK, hist ? (size_t)k * sizeof(W) : 0, s>>>(a, hist);
+        JET_LAUNCH_CHECK();
+        int h = prof_begin(s);
+        unsigned grid = grid_persistent((int64_t)L.n * L.group / 4 + 1, 16);
+        switch (L.group) {
+            case 4: k_update_small<4, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); k_update_small<4, true, O, E, W><<<grid, BLOCK, 0, s>>>(a);
+                    k_mark_neighbors<4, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 8: k_update_small<8, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); k_update_small<8, true, O, E, W><<<grid, BLOCK, 0, s>>>(a);
+                    k_mark_neighbors<8, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 16: k_update_small<16, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); k_update_small<16, true, O, E, W><<<grid, BLOCK, 0, s>>>(a);
+                     k_mark_neighbors<16, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            default: k_update_small<32, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); k_update_small<32, true, O, E, W><<<grid, BLOCK, 0, s>>>(a);
+                     k_mark_neighbors<32, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+        }
+        JET_LAUNCH_CHECK();
+        if (L.n_hub > 0) {
+            // the subtract pass must finish before any add: two launches
+            k_update_small_hub<false, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a);
+            k_update_small_hub<true, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a);
+            JET_LAUNCH_CHECK();
+        }
+        build_tables(L, 1, &dev.p->large);
+        prof_end(h, PK_UPDATE, 0, s);
+        k_cut_after<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(a);
+        k_finalize<O, E, W><<<1, 1024, 0, s>>>(a, e.hres);
+        JET_LAUNCH_CHECK();
+        e.sync();
+        IterResult r = *e.hres;
+        if (r.err) throw JetError{JET_ERR_OVERFLOW, "connectivity table update exceeded its bounds"};
+        return r;
+    }
+
+    W total_cut(const Level<O, E, W>& L, const part_t* part) {
+        W* out = e.template dslot<W>(50);
+        JET_CUDA(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
+        unsigned grid = grid_persistent((int64_t)L.n * L.group, 16);
+        switch (L.group) {
+            case 4: k_total_cut<4, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); break;
+            case 8: k_total_cut<8, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); break;
+            case 16: k_total_cut<16, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); break;
+            default: k_total_cut<32, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); break;
+        }
+        JET_LAUNCH_CHECK();
+        JET_CUDA(cudaMemcpyAsync(&e.hscal[0], out, sizeof(W), cudaMemcpyDeviceToHost, s));
+        e.sync();
+        return *(W*)&e.hscal[0];
+    }
+
+    void part_sizes(const Level<O, E, W>& L, const part_t* part, W* sizes) {
+        JET_CUDA(cudaMemsetAsync(sizes, 0, sizeof(W) * k, s));
+        int hist = (size_t)k * sizeof(W) <= 32 * 1024;
+        k_part_sizes<O, W><<<grid_persistent(L.n, 8), BLOCK, hist ? (size_t)k * sizeof(W) : 0, s>>>(L.n, L.vw, part, k, sizes, hist);
+        JET_LAUNCH_CHECK();
+    }
+
+    W sum_vw(const Level<O, E, W>& L) {
+        W* out = e.template dslot<W>(51);
+        JET_CUDA(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
+        k_sum<W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(L.vw, L.n, out);
+        JET_LAUNCH_CHECK();
+        JET_CUDA(cudaMemcpyAsync(&e.hscal[0], out, sizeof(W), cudaMemcpyDeviceToHost, s));
+        e.sync();
+        return *(W*)&e.hscal[0];
+    }
+
+    W max_of_sizes(const W* sizes) {
+        std::vector<W> h(k);
+        JET_CUDA(cudaMemcpyAsync(h.data(), sizes, sizeof(W) * k, cudaMemcpyDeviceToHost, s));
+        e.sync();
+        W mx = 0;
+        for (W x : h) if (x > mx) mx = x;
+        return mx;
+    }
+
+    void check_parts(const Level<O, E, W>& L, const part_t* part) {
+        int* err = e.template dslot<int>(52);
+        JET_CUDA(cudaMemsetAsync(err, 0, sizeof(int64_t), s));
+        k_check_parts<<<grid_persistent(L.n, 8), BLOCK, 0, s>>>((int64_t)L.n, part, k, err);
+        JET_LAUNCH_CHECK();
+        JET_CUDA(cudaMemcpyAsync(&e.hscal[0], err, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        e.sync();
+        if (*(int*)&e.hscal[0]) throw JetError{JET_ERR_INVALID, "part id out of range"};
+    }
+
+    // Sets up refinement state for a level (problem values and tables).
+    struct Prob {
+        W opt, size_max, imb_max;
+    };
+    Prob begin_level(const Level<O, E, W>& L, part_t* best_part, double imb) {
+        if (!best.init) {
+            check_parts(L, best_part);
+            best.cut = total_cut(L, best_part);
+            part_sizes(L, best_part, sizes_best.p);
+            best.total_size = sum_vw(L);
+        }
+        Prob pb;
+        O opt = (O)(((O)best.total_size + k - 1) / k);  // optimal_size, ordinal arithmetic (src/part_stat.hpp:111-114)
+        O size_max = (O)((double)opt * imbalance_guard(imb));
+        pb.opt = opt;
+        pb.size_max = size_max;
+        pb.imb_max = (W)size_max - (W)opt;
+        if (!best.init) {
+            best.init = true;
+            W mx = max_of_sizes(sizes_best.p);
+            best.total_imb = mx > pb.opt ? mx - pb.opt : 0;
+            if (verbose)
+                printf("Initial %lld %.6f %lld\n", (long long)(best.cut / 2), (double)best.total_imb / (double)pb.opt, (long long)L.n);
+        }
+        curr = best;
+        JET_CUDA(cudaMemcpyAsync(sizes_curr.p, sizes_best.p, sizeof(W) * k, cudaMemcpyDeviceToDevice, s));
+        JET_CUDA(cudaMemcpyAsync(part_work.p, best_part, sizeof(part_t) * L.n, cudaMemcpyDeviceToDevice, s));
+        init_conn(L);
+        return pb;
+    }
+    static double imbalance_guard(double imb) { return imb; }
+
+    // One iteration body of jet_refine (src/jet_refiner.hpp:1106-1120).
+    int iterate(const Level<O, E, W>& L, const Prob& pb, double filter_ratio, int& balance_counter, int& lab_counter) {
+        int kind;
+        if (curr.total_imb <= pb.imb_max) {
+            lp(L, filter_ratio);
+            balance_counter = 0;
+            lab_counter++;
+            kind = 0;
+        } else {
+            if (balance_counter < 2) { weak(L, pb.opt, pb.size_max); kind = 1; }
+            else { strong(L, pb.opt, pb.size_max); kind = 2; }
+            balance_counter++;
+        }
+        IterResult r = perform_moves(L);
+        curr.cut -= (W)r.cut_change;
+        W mx = (W)r.max_part;
+        curr.total_imb = mx > pb.opt ? mx - pb.opt : 0;
+        last_moves = r.nmoves;
+        total_iters++;
+        return kind;
+    }
+    int64_t last_moves = 0;
+
+    void save_best(const Level<O, E, W>& L, part_t* best_part) {
+        best = curr;
+        JET_CUDA(cudaMemcpyAsync(sizes_best.p, sizes_curr.p, sizeof(W) * k, cudaMemcpyDeviceToDevice, s));
+        JET_CUDA(cudaMemcpyAsync(best_part, part_work.p, sizeof(part_t) * L.n, cudaMemcpyDeviceToDevice, s));
+    }
+
+    // jet_refine, src/jet_refiner.hpp:1050-1142.  best_part in/out.
+    jet_level_stats_c refine(const Level<O, E, W>& L, part_t* best_part, double imb, double tol, bool ultra) {
+        auto t0 = clk::now();
+        Prob pb = begin_level(L, best_part, imb);
+        auto t1 = clk::now();
+        std::vector<double> temps;
+        if (ultra) { for (double t = 0.85; t > 0; t -= 0.05) temps.push_back(t); }
+        else if (L.uniform) temps.push_back(0.25);
+        else temps.push_back(0.75);
+        int iter_count = 0, balance_counter = 0, lab_counter = 0;
+        for (double fr : temps) {
+            int count = 0;
+            while (count++ <= 11) {
+                iter_count++;
+                iterate(L, pb, fr, balance_counter, lab_counter);
+                if (best.total_imb > pb.imb_max && curr.total_imb < best.total_imb) {
+                    save_best(L, best_part);
+                    count = 0;
+                } else if (curr.cut < best.cut && (curr.total_imb <= pb.imb_max || curr.total_imb <= best.total_imb)) {
+                    if ((double)curr.cut < tol * (double)best.cut) count = 0;
+                    save_best(L, best_part);
+                }
+            }
+        }
+        e.sync();
+        jet_level_stats_c cl;
+        cl.edge_cut = (int64_t)(best.cut / 2);
+        cl.imb = (double)best.total_imb / (double)pb.opt;
+        cl.num_edges = (uint64_t)L.m;
+        cl.num_vertices = (uint64_t)L.n;
+        cl.total_ref_time = since(t0);
+        cl.iterations_time = since(t1);
+        cl.total_iterations = iter_count;
+        cl.lp_iterations = lab_counter;
+        return cl;
+    }
+};
+
+// ---------------------------------------------------------------- partition
+template <class O, class E, class W>
+struct GraphIn {
+    O n;
+    E m;
+    const E* row;
+    const O* adj;
+    const W* val;
+    const W* vw;
+    bool uniform;
+};
+
+// metis_init, src/initial_partition.hpp:92-114: values pass through `int`
+// as in the reference, then widen to this Metis build's 64-bit idx_t.
+template <class O, class E, class W>
+void metis_coarsest(const Level<O, E, W>& L, part_t k, double imb, part_t* part_dev, cudaStream_t s) {
+    std::vector<E> row(L.n + 1);
+    std::vector<O> adj(L.m);
+    std::vector<W> val(L.m), vw(L.n);
+    JET_CUDA(cudaMemcpyAsync(row.data(), L.row, sizeof(E) * (L.n + 1), cudaMemcpyDeviceToHost, s));
+    if (L.m) {
+        JET_CUDA(cudaMemcpyAsync(adj.data(), L.adj, sizeof(O) * L.m, cudaMemcpyDeviceToHost, s));
+        JET_CUDA(cudaMemcpyAsync(val.data(), L.val, sizeof(W) * L.m, cudaMemcpyDeviceToHost, s));
+    }
+    JET_CUDA(cudaMemcpyAsync(vw.data(), L.vw, sizeof(W) * L.n, cudaMemcpyDeviceToHost, s));
+    JET_CUDA(cudaStreamSynchronize(s));
+    metis_idx_t n = L.n, ncon = 1, nparts = k, obj = 0;
+    std::vector<metis_idx_t> xadj(L.n + 1), madj(L.m), madjw(L.m), mvw(L.n), pm(L.n, 0);
+    for (O i = 0; i <= L.n; i++) xadj[i] = (int)row[i];
+    for (E j = 0; j < L.m; j++) { madj[j] = (int)adj[j]; madjw[j] = (int)val[j]; }
+    for (O i = 0; i < L.n; i++) mvw[i] = (int)vw[i];
+    metis_real_t ub = (metis_real_t)imb;
+    int ret = METIS_PartGraphKway(&n, &ncon, xadj.data(), madj.data(), mvw.data(), nullptr, madjw.data(), &nparts, nullptr,
+                                  &ub, nullptr, &obj, pm.data());
+    if (ret != 1) throw JetError{JET_ERR_METIS, "Metis could not partition coarsest graph"};
+    std::vector<part_t> p(L.n);
+    for (O i = 0; i < L.n; i++) p[i] = (part_t)pm[i];
+    JET_CUDA(cudaMemcpyAsync(part_dev, p.data(), sizeof(part_t) * L.n, cudaMemcpyHostToDevice, s));
+    JET_CUDA(cudaStreamSynchronize(s));
+}
+
+struct Cfg {
+    int alg;
+    part_t k;
+    double imb;
+    double tol;
+    bool ultra;
+    bool verbose;
+};
+
+template <class O, class E, class W>
+W run_partition(Engine<O, E, W>& eng, const Cfg& cfg, const GraphIn<O, E, W>& in, uint64_t seed, part_t* part_out,
+                jet_stats_c* st) {
+    cudaStream_t s = eng.s;
+    auto t_start = clk::now();
+    double meas[JET_NUM_MEASUREMENTS] = {0};
+    part_t k = cfg.k;
+    std::vector<std::unique_ptr<Level<O, E, W>>> levels;
+    levels.emplace_back(new Level<O, E, W>());
+    Level<O, E, W>& L0 = *levels[0];
+    L0.n = in.n; L0.m = in.m; L0.row = in.row; L0.adj = in.adj; L0.val = in.val; L0.vw = in.vw; L0.uniform = in.uniform;
+    eng.prepare_level(L0);
+    // coarsening cutoff, src/partitioner.hpp:88-94
+    int cutoff = k * 8;
+    if (cutoff > 1024) { cutoff = k * 2; cutoff = cutoff > 1024 ? cutoff : 1024; }
+    O min_allowed = cutoff / 4;
+    int alg = cfg.alg;
+    if (alg < 0 || alg > 2) alg = 0;
+    DBuf<O> skey(L0.m > 0 ? L0.m : 1, s);
+    DBuf<W> sval(L0.m > 0 ? L0.m : 1, s);
+    // level loop, src/contract.hpp:494-533
+    while (levels.back()->n > (O)cutoff) {
+        Level<O, E, W>& cur = *levels.back();
+        DBuf<O> map(cur.n, s);
+        auto tm = clk::now();
+        int h = prof_begin(s);
+        O nc = eng.coarsen_map(cur, alg, seed, (int)levels.size(), map.p, nullptr, meas);
+        prof_end(h, PK_HEC, 0, s);
+        meas[M_MAP] += since(tm);
+        if (nc < min_allowed) break;
+        auto tb = clk::now();
+        std::unique_ptr<Level<O, E, W>> next(new Level<O, E, W>());
+        h = prof_begin(s);
+        eng.contract(cur, map.p, nc, *next, &skey, &sval);
+        prof_end(h, PK_CONTRACT, 0, s);
+        next->map = std::move(map);
+        eng.prepare_level(*next);
+        meas[M_BUILD] += since(tb);
+        levels.push_back(std::move(next));
+        if (levels.size() > 200) break;
+    }
+    skey.release();
+    sval.release();
+    eng.sync();
+    double t_coarsen = since(t_start);
+    // initial partition
+    auto ti = clk::now();
+    Level<O, E, W>& coarsest = *levels.back();
+    const int64_t coarsest_n = (int64_t)coarsest.n;
+    DBuf<part_t> pa(L0.n > 0 ? L0.n : 1, s), pb(L0.n > 0 ? L0.n : 1, s);
+    metis_coarsest(coarsest, k, cfg.imb, pa.p, s);
+    meas[M_INITPARTITION] += since(ti);
+    // uncoarsen, src/uncoarsen.hpp:88-125
+    auto tr = clk::now();
+    Refiner<O, E, W> ref(eng, L0.n, (int64_t)L0.m, k);
+    ref.verbose = cfg.verbose;
+    part_t* cur_part = pa.p;
+    part_t* other = pb.p;
+    int nl = (int)levels.size();
+    if (st) st->num_levels = nl;
+    for (int l = nl - 1; l >= 0; l--) {
+        jet_level_stats_c cl = ref.refine(*levels[l], cur_part, cfg.imb, cfg.tol, cfg.ultra);
+        int idx = nl - 1 - l;
+        if (st && idx < JET_MAX_LEVELS) st->levels[idx] = cl;
+        if (l > 0) {
+            Level<O, E, W>& fine = *levels[l - 1];
+            k_project<O><<<grid_persistent(fine.n, 16), BLOCK, 0, s>>>(fine.n, levels[l]->map.p, cur_part, other);
+            JET_LAUNCH_CHECK();
+            std::swap(cur_part, other);
+            if (l - 1 > 0) { levels[l].reset(); }
+        }
+    }
+    eng.sync();
+    meas[M_REFINE] += since(tr);
+    JET_CUDA(cudaMemcpyAsync(part_out, cur_part, sizeof(part_t) * L0.n, cudaMemcpyDeviceToDevice, s));
+    W cut_half = ref.best.cut / 2;
+    if (st) {
+        std::vector<W> hs(k);
+        JET_CUDA(cudaMemcpyAsync(hs.data(), ref.sizes_best.p, sizeof(W) * k, cudaMemcpyDeviceToHost, s));
+        eng.sync();
+        W largest = 0, smallest = ref.best.total_size;
+        for (W x : hs) { if (x > largest) largest = x; if (x < smallest) smallest = x; }
+        double opt = (double)(O)(((O)ref.best.total_size + k - 1) / k);
+        st->edge_cut = (int64_t)cut_half;
+        st->imb_ratio = (double)largest / opt;
+        st->largest_part = (int64_t)largest;
+        st->smallest_part = (int64_t)smallest;
+        st->coarsest_vertices = coarsest_n;
+        st->refine_iterations = ref.total_iters;
+        meas[M_COARSEN] = t_coarsen;
+        meas[M_TOTAL] = since(t_start);
+        for (int i = 0; i < JET_NUM_MEASUREMENTS; i++) st->measurements[i] = meas[i];
+    }
+    eng.sync();
+    return cut_half;
+}
+
+}  // namespace jetb
