@@ -1,0 +1,291 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 Jet partitioner.
+
+A step is one complete multilevel partition of one graph (coarsening,
+Metis on the coarsest graph, Jet refinement and projection back to the
+finest level) with the graph already resident in HBM.  The default workload
+is the 3D 7-point grid 128^3 (2,097,152 vertices, 6,242,304 edges, weights
+uniform in [1, 10] from seed 1), k = 64, HEC coarsening, imbalance 1.03.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+With --gpus N > 1 (launched by torch.distributed.run) every rank partitions
+its own replica of the graph (independent work, no collective on the data
+path); the value is the whole job's graphs/s over the max-over-ranks time.
+--impl reference times the CPU oracle (a restatement of the reference's
+algorithm; the reference itself needs Kokkos and cannot be built here) on the
+host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "jet-partitioner-official-fork_b200")
+
+
+def load_pkg():
+    spec = importlib.util.spec_from_file_location("jet_b200", os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["jet_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+WORKLOADS = {
+    "grid3d128": dict(desc="3D 7-point grid 128^3, edge weights uniform in [1,10] (seed 1)", k=64, alg=1, imb=1.03,
+                      tier="i32", make=lambda gr, dev: gr.grid3d(128, 128, 128, weighted=True, seed=1, tier="i32", device=dev)),
+    "grid2d256": dict(desc="2D 4-neighbour grid 256x256, unit weights", k=32, alg=1, imb=1.03, tier="i32",
+                      make=lambda gr, dev: gr.grid2d(256, 256, weighted=False, tier="i32", device=dev)),
+    "rmat24": dict(desc="R-MAT 2^24, edge factor 8 (0.57/0.19/0.19/0.05), symmetrised, de-duplicated, unit weights",
+                   k=256, alg=0, imb=1.10, tier="big",
+                   make=lambda gr, dev: gr.rmat(24, 8, seed=1, tier="big", device=dev)),
+    "rmat18": dict(desc="R-MAT 2^18, edge factor 8 (0.57/0.19/0.19/0.05), symmetrised, de-duplicated, unit weights",
+                   k=256, alg=0, imb=1.10, tier="big",
+                   make=lambda gr, dev: gr.rmat(18, 8, seed=1, tier="big", device=dev)),
+}
+ALG_NAME = {0: "2-hop matching", 1: "HEC", 2: "matching"}
+PART_FN = {"i32": "partition", "big": "partition_big", "biggest": "partition_biggest"}
+HOST_FN = {"i32": "partition_host", "big": "partition_host_big", "biggest": "partition_host_biggest"}
+ITEM = {"i32": (4, 4, 4), "big": (4, 8, 8), "biggest": (8, 8, 8)}  # ordinal, offset, weight bytes
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(prefix="clocks", suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        for ln in open(self.path):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        mhz = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def oracle_partition(g, wl, seed):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    og = oracle.G.from_csr(g.to("cpu"))
+    t = time.perf_counter()
+    part, cut, st = oracle.partition(og, wl["k"], alg=wl["alg"], imb=wl["imb"], seed=seed)
+    return time.perf_counter() - t, cut, st.imb
+
+
+def run_reference(args, wl, rank):
+    """CPU oracle of the reference algorithm, one full partition per step."""
+    if rank != 0:
+        return
+    jet = load_pkg()
+    g = wl["make"](jet.graphs, "cpu")
+    for s in range(args.warmup):
+        oracle_partition(g, wl, seed=100 + s)
+    times, cuts, imbs = [], [], []
+    for s in range(args.steps):
+        dt, cut, imb = oracle_partition(g, wl, seed=1 + s)
+        times.append(dt)
+        cuts.append(cut)
+        imbs.append(imb)
+    total = sum(times)
+    value = args.steps / total
+    line = {
+        "impl": "reference", "metric": "graphs/sec", "value": value, "unit": "graphs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": wl["tier"], "data": "synthetic",
+        "config": config_of(args, wl, g),
+        "edges_per_s": value * g.nnz / 2, "cut_median": statistics.median(cuts), "imbalance_max": max(imbs),
+        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": 1, "kind": "port",
+                         "sample": "%d full partitions of the workload on one host thread (oracle/jet_oracle.cpp)" % args.steps},
+        "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, wl, g):
+    return {"workload": args.workload, "graph": wl["desc"], "n": g.n, "undirected_edges": g.nnz // 2, "k": wl["k"],
+            "coarsening": ALG_NAME[wl["alg"]], "imbalance": wl["imb"], "tier": wl["tier"],
+            "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas x%d" % args.gpus}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="grid3d128", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, wl, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    jet = load_pkg()
+    dev = torch.device("cuda", local)
+    g = wl["make"](jet.graphs, dev)
+    cfg = jet.config_t(coarsening_alg=wl["alg"], num_parts=wl["k"], max_imb_ratio=wl["imb"])
+    part_fn = getattr(jet, PART_FN[wl["tier"]])
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)
+
+    for s in range(args.warmup):
+        part_fn(cfg, g, seed=100 + s)
+    torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    jet.prof_enable(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = jet.launch_count()
+    times, cuts, imbs = [], [], []
+    for s in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        part, cut, exp = part_fn(cfg, g, seed=1 + s, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        cuts.append(cut)
+        imbs.append(exp.imb_ratio)
+    launches = jet.launch_count() - launches0
+    clk = clocks.stop()
+    prof = jet.prof_read()
+    jet.prof_enable(False)
+    total_ms = sum(times)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    max_total_ms = float(t.item())
+    value = ws * args.steps / (max_total_ms / 1000.0)
+
+    # end to end through the C ABI with host buffers (copies in the timed region)
+    host_fn = getattr(jet, HOST_FN[wl["tier"]])
+    gh = g.to("cpu")
+    gh = jet.graphs.CSRGraph(gh.n, gh.row.pin_memory(), gh.adj.pin_memory(), gh.val.pin_memory(), gh.vw.pin_memory(),
+                             gh.uniform, gh.tier)
+    if args.e2e_steps > 0:
+        host_fn(cfg, gh, seed=7)
+    e2e_times = []
+    for s in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        host_fn(cfg, gh, seed=1 + s)
+        e2e_times.append(time.perf_counter() - t0)
+    ob, eb, wb = ITEM[wl["tier"]]
+    h2d = (g.n + 1) * eb + g.nnz * (ob + wb) + g.n * wb
+    d2h = g.n * 4
+    e2e_value = ws * len(e2e_times) / sum(e2e_times) if e2e_times else None
+
+    if rank != 0:
+        if ws > 1:
+            dist.destroy_process_group()
+        return
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    # dominant kernel class with an algorithmic byte model
+    ranked = sorted(((v["ms"], nm) for nm, v in prof.items() if v["bytes"] > 0 and v["launches"] > 0), reverse=True)
+    roof = None
+    if ranked:
+        nm = ranked[0][1]
+        v = prof[nm]
+        per_launch_ms = v["ms"] / v["launches"]
+        achieved = (v["bytes"] / v["launches"]) / (per_launch_ms / 1000.0) / 1e9
+        roof = {"kernel": nm, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "bytes_per_launch": v["bytes"] / v["launches"], "ms_per_launch": per_launch_ms,
+                "launches": v["launches"]}
+    cpu_base = None
+    if ws == 1 and not args.no_cpu_baseline:
+        dt, ocut, oimb = oracle_partition(g, wl, seed=1)
+        cpu_base = {"value": 1.0 / dt, "unit": "graphs/s", "cores": 1, "kind": "port",
+                    "sample": "one full partition of the same graph on one host thread (oracle/jet_oracle.cpp), cut %d" % ocut}
+    sorted_t = sorted(times)
+    line = {
+        "metric": "graphs/sec", "value": value, "unit": "graphs/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": wl["tier"], "data": "synthetic", "config": config_of(args, wl, g),
+        "edges_per_s": value * g.nnz / 2,
+        "latency_ms": {"p50": statistics.median(times), "p99": sorted_t[min(len(sorted_t) - 1, int(0.99 * len(sorted_t)))]},
+        "cut_median": statistics.median(cuts), "imbalance_max": max(imbs),
+        "e2e": {"value": e2e_value, "unit": "graphs/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": roof,
+        "kernel_classes_ms": {nm: round(v["ms"], 3) for nm, v in prof.items()},
+        "cpu_baseline": cpu_base,
+        "clocks": clk,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -163,6 +163,9 @@ int jet_device_ok(void);
 int jet_prof_enable(int on);
 int jet_prof_read(double* ms, double* bytes, int64_t* launches);
 
+/* Number of CUDA kernels this library has launched in this process. */
+int64_t jet_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

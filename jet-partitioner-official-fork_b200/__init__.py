@@ -53,7 +53,7 @@ MEASUREMENT_NAMES = [  # header/experiment_data.hpp:77-98
 EXPORTED_SYMBOLS = [
     "jet_partition_i32", "jet_partition_big", "jet_partition_biggest", "jet_coarsen_map", "jet_contract",
     "jet_conn_build", "jet_refine_iters", "jet_refine_level", "jet_pstat", "jet_project", "jet_version",
-    "jet_last_error", "jet_device_ok", "jet_prof_enable", "jet_prof_read",
+    "jet_last_error", "jet_device_ok", "jet_prof_enable", "jet_prof_read", "jet_launch_count",
 ]
 
 
@@ -106,6 +106,7 @@ def load(build_if_missing: bool = False):
     lib = ctypes.CDLL(LIB_PATH)
     lib.jet_version.restype = ctypes.c_char_p
     lib.jet_last_error.restype = ctypes.c_char_p
+    lib.jet_launch_count.restype = ctypes.c_int64
     _lib = lib
     return lib
 
@@ -418,6 +419,11 @@ def project(cmap: torch.Tensor, coarse_part: torch.Tensor, tier: str = "i32") ->
     _check(load().jet_project(TIER_ID[tier], ctypes.c_int64(cmap.numel()), _ptr(cmap), _ptr(coarse_part), _ptr(fine),
                               _stream_ptr()))
     return fine
+
+
+def launch_count() -> int:
+    """Kernels launched by the library so far in this process."""
+    return int(load().jet_launch_count())
 
 
 def prof_enable(on: bool = True):

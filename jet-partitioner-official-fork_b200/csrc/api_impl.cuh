@@ -52,7 +52,7 @@ template <class O, class E, class W>
 void validate(Engine<O, E, W>& eng, O n, E m, const E* row, const O* adj, const W* val, const W* vw) {
     int* err = eng.template dslot<int>(60);
     JET_CUDA(cudaMemsetAsync(err, 0, sizeof(int64_t), eng.s));
-    k_validate<O, E, W><<<grid_persistent(n > 0 ? n : 1, 8), BLOCK, 0, eng.s>>>(n, m, row, adj, val, vw, err);
+    k_validate<O, E, W><<<grid_persistent(n > 0 ? n : 1, 8), BLOCK, 0, eng.s>>>(n, m, row, adj, val, vw, err); count_launch();
     JET_LAUNCH_CHECK();
     JET_CUDA(cudaMemcpyAsync(&eng.hscal[0], err, sizeof(int64_t), cudaMemcpyDeviceToHost, eng.s));
     eng.sync();
@@ -177,7 +177,7 @@ void pstat_impl_dev(Engine<O, E, W>& eng, O n, E m, const E* row, const O* adj, 
     W cut = ref.total_cut(L, part);
     DBuf<W> per(k, s);
     per.zero();
-    k_cut_per_part<O, E, W><<<grid_persistent(n, 8), BLOCK, 0, s>>>(L.view(), part, per.p);
+    k_cut_per_part<O, E, W><<<grid_persistent(n, 8), BLOCK, 0, s>>>(L.view(), part, per.p); count_launch();
     JET_LAUNCH_CHECK();
     std::vector<W> hper(k), hs(k);
     JET_CUDA(cudaMemcpyAsync(hper.data(), per.p, sizeof(W) * k, cudaMemcpyDeviceToHost, s));
@@ -187,7 +187,7 @@ void pstat_impl_dev(Engine<O, E, W>& eng, O n, E m, const E* row, const O* adj, 
     ref.init_conn(L);
     long long* cc = eng.template dslot<long long>(61);
     JET_CUDA(cudaMemsetAsync(cc, 0, sizeof(int64_t), s));
-    k_comm_count<O, E, W><<<grid_persistent(n, 8), BLOCK, 0, s>>>(L.view(), part, ref.coff.p, ref.slots.p, ref.csize.p, cc);
+    k_comm_count<O, E, W><<<grid_persistent(n, 8), BLOCK, 0, s>>>(L.view(), part, ref.coff.p, ref.slots.p, ref.csize.p, cc); count_launch();
     JET_LAUNCH_CHECK();
     JET_CUDA(cudaMemcpyAsync(&eng.hscal[1], cc, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     eng.sync();
@@ -339,7 +339,7 @@ struct Tier {
         return guarded([&]() -> int {
             cudaStream_t s = pick_stream(stream);
             if (n_fine > 0) {
-                k_project<O><<<grid_persistent(n_fine, 16), BLOCK, 0, s>>>((O)n_fine, (const O*)map, coarse, fine);
+                k_project<O><<<grid_persistent(n_fine, 16), BLOCK, 0, s>>>((O)n_fine, (const O*)map, coarse, fine); count_launch();
                 JET_LAUNCH_CHECK();
             }
             JET_CUDA(cudaStreamSynchronize(s));

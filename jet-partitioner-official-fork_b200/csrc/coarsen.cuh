@@ -150,6 +150,116 @@ __global__ void k_hec_compact(O n, const O* perm, const O* perm_len, const O* vc
     }
 }
 
+// ---------------------------------------------------------------- HEC, in-order semantics
+// The reference's aggregation rounds (src/heuristics.hpp:101-126) executed in
+// index order settle every vertex within two rounds, and both rounds have a
+// data-parallel formulation that yields exactly the in-order result:
+//
+// Round 1 (swap = 1) processes A = {u : hn[u] <= u}.  Every u in A is still
+// free at its turn (claims go to smaller indices), and it ends in the
+// aggregate found by following hn through A: the chain stops at t with
+// hn[t] == t (root t) or at h = hn[t] outside A (h is claimed as a partner and
+// becomes the root).  Resolved by pointer jumping.
+//
+// Round 2 (swap = 0) processes the rest, B, all with hn[u] > u, in index order.
+// u is claimed by its smallest free child (a free w in B with hn[w] == u) if
+// one exists; otherwise u is free and pairs with hn[u] when it is its parent's
+// smallest free child and the parent is in B, else joins the parent's
+// aggregate.  "free" is a NOR over children, evaluated bottom-up in one pass in
+// which the last child to finish continues with the parent.
+template <class O>
+__device__ __forceinline__ O hec_enc(O root) { return (O)(-2) - root; }  // terminal marker (< -1)
+
+template <class O>
+__global__ void k_hec_p1_init(O n, const O* hn, O* nxt, O* vcmap) {
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+        O u = (O)x;
+        O h = hn[u];
+        if (h > u) { nxt[u] = (O)-1; continue; }  // not in A
+        if (h == u) { nxt[u] = hec_enc<O>(u); continue; }
+        if (hn[h] <= h) { nxt[u] = h; continue; }  // parent inside A
+        nxt[u] = hec_enc<O>(h);
+        vcmap[h] = h;  // h is claimed as a partner: root of its aggregate
+    }
+}
+
+template <class O>
+__global__ void k_hec_p1_jump(O n, O* nxt, int* changed) {
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+        O p = ld_cg(&nxt[x]);
+        if (p < 0) continue;
+        O q = ld_cg(&nxt[p]);
+        if (q != p) { st_v(&nxt[x], q); *changed = 1; }
+    }
+}
+
+template <class O>
+__global__ void k_hec_p1_final(O n, const O* nxt, O* vcmap) {
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+        O e = nxt[x];
+        if (e < -1) vcmap[x] = (O)(-2) - e;
+    }
+}
+
+template <class O>
+__global__ void k_hec_p2_count(O n, const O* hn, const O* vcmap, uint8_t* inB, O* cnt, O* min_free, int* has_free) {
+    const O MAXV = ord_max<O>();
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+        O u = (O)x;
+        bool b = vcmap[u] == MAXV;
+        inB[u] = b;
+        min_free[u] = MAXV;
+        has_free[u] = 0;
+        if (b) {
+            O v = hn[u];
+            if (vcmap[v] == MAXV) atomic_add(&cnt[v], (O)1);
+        }
+    }
+}
+
+template <class O>
+__device__ __forceinline__ void atomic_min_o(int32_t* p, int32_t v) { atomicMin((int*)p, v); }
+template <class O>
+__device__ __forceinline__ void atomic_min_o(int64_t* p, int64_t v) { atomicMin((long long*)p, (long long)v); }
+
+template <class O>
+__global__ void k_hec_p2_walk(O n, const O* hn, const uint8_t* inB, O* cnt, O* min_free, int* has_free) {
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+        O cur = (O)x;
+        if (!inB[cur] || ld_cg(&cnt[cur]) != 0) continue;  // only leaves start a walk
+        while (true) {
+            bool is_free = ld_cg(&has_free[cur]) == 0;
+            O v = hn[cur];
+            if (!inB[v]) break;
+            if (is_free) {
+                atomic_min_o<O>(&min_free[v], cur);
+                atomicOr(&has_free[v], 1);
+            }
+            __threadfence();
+            if (atomic_add(&cnt[v], (O)-1) != 1) break;  // another child finishes v later
+            __threadfence();
+            cur = v;
+        }
+    }
+}
+
+template <class O>
+__global__ void k_hec_p2_roots(O n, const O* hn, const uint8_t* inB, const O* min_free, const int* has_free, O* vcmap) {
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
+        O u = (O)x;
+        if (!inB[u]) continue;
+        O root;
+        if (has_free[u]) {
+            root = min_free[u];
+        } else {
+            O v = hn[u];
+            if (inB[v]) root = (min_free[v] == u) ? u : min_free[v];
+            else root = vcmap[v];
+        }
+        vcmap[u] = root;
+    }
+}
+
 // Roots (vcmap[u] == u) are numbered in index order; others take their
 // root's number (src/heuristics.hpp:147-165, :655-665).
 template <class O>
@@ -275,13 +385,17 @@ __global__ void __launch_bounds__(1024) k_pick_match_hub(GView<O, E, W> g, const
     }
 }
 
-// Commit rounds, src/heuristics.hpp:462-501.
+// Commit rounds, src/heuristics.hpp:462-501.  Part 1 marks inactive
+// vertices; in part 2 an inactive v goes to the first active proposer in
+// index order (what the reference's in-order pass yields), found with
+// atomicMin so the outcome does not depend on thread timing.
 template <class O>
-__global__ void k_commit1(O n, const O* perm, const O* perm_len, const O* hn, O* vcmap, int r) {
+__global__ void k_commit1(O n, const O* perm, const O* perm_len, const O* hn, O* vcmap, O* winner, int r) {
     const O MAXV = ord_max<O>();
     O len = perm ? *perm_len : n;
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < len; x += (int64_t)gridDim.x * blockDim.x) {
         O u = perm ? perm[x] : (O)x;
+        winner[u] = MAXV;
         O v = hn[u];
         if (v == MAXV || vcmap[u] != MAXV) continue;
         bool cond = r > 0 ? (pod_hash((O)(u + r)) < pod_hash((O)(v + r))) : (u < v);
@@ -289,15 +403,29 @@ __global__ void k_commit1(O n, const O* perm, const O* perm_len, const O* hn, O*
     }
 }
 template <class O>
-__global__ void k_commit2(O n, const O* perm, const O* perm_len, const O* hn, O* vcmap) {
+__global__ void k_commit2a(O n, const O* perm, const O* perm_len, const O* hn, const O* vcmap, O* winner) {
     const O MAXV = ord_max<O>();
     O len = perm ? *perm_len : n;
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < len; x += (int64_t)gridDim.x * blockDim.x) {
         O u = perm ? perm[x] : (O)x;
         O v = hn[u];
-        if (v == MAXV || ld_cg(&vcmap[u]) != MAXV) continue;
-        O cv = u < v ? u : v;
-        if (atomic_cas(&vcmap[v], MAXV - 1, cv) == MAXV - 1) st_v(&vcmap[u], cv);
+        if (v == MAXV || vcmap[u] != MAXV) continue;
+        if (vcmap[v] == MAXV - 1) atomic_min_o<O>(&winner[v], u);
+    }
+}
+template <class O>
+__global__ void k_commit2(O n, const O* perm, const O* perm_len, const O* hn, O* vcmap, const O* winner) {
+    const O MAXV = ord_max<O>();
+    O len = perm ? *perm_len : n;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < len; x += (int64_t)gridDim.x * blockDim.x) {
+        O u = perm ? perm[x] : (O)x;
+        O v = hn[u];
+        if (v == MAXV || vcmap[u] != MAXV) continue;
+        if (winner[v] == u) {
+            O cv = u < v ? u : v;
+            vcmap[v] = cv;
+            vcmap[u] = cv;
+        }
     }
 }
 template <class O>

@@ -17,8 +17,35 @@ namespace jetb {
 
 static constexpr int CT_S1_DU = 256, CT_S1_SLOTS = 512, CT_S1_THREADS = 128;
 static constexpr int CT_S2_DU = 4096, CT_S2_SLOTS = 8192, CT_S2_THREADS = 512;
+__host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
+// hash table (slots) plus a sort buffer of slots/2 entries (a row in the bin
+// has at most slots/2 distinct neighbours)
 template <class O, class W>
-constexpr size_t contract_smem_bytes(int slots) { return (((size_t)slots * sizeof(O) + 15) & ~(size_t)15) + (size_t)slots * sizeof(W); }
+constexpr size_t contract_smem_bytes(int slots) {
+    return align16((size_t)slots * sizeof(O)) + align16((size_t)slots * sizeof(W)) + align16((size_t)(slots / 2) * sizeof(O)) +
+           (size_t)(slots / 2) * sizeof(W);
+}
+
+// Sorts P (a power of two) key/value pairs in shared memory by key.
+template <int THREADS, class K, class V>
+__device__ __forceinline__ void block_bitonic_sort(K* key, V* val, int P) {
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += THREADS) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    bool up = (i & k) == 0;
+                    K a = key[i], b = key[ixj];
+                    if ((a > b) == up) {
+                        key[i] = b; key[ixj] = a;
+                        V t = val[i]; val[i] = val[ixj]; val[ixj] = t;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
 
 template <class O, class E, class W>
 __global__ void k_contract_count(GView<O, E, W> g, const O* map, O* cnt, E* du, W* cvw) {
@@ -149,7 +176,9 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
                                                           O* ucnt) {
     extern __shared__ __align__(16) unsigned char ct_smem[];
     O* keys = (O*)ct_smem;
-    W* vals = (W*)(ct_smem + (((size_t)SLOTS * sizeof(O) + 15) & ~(size_t)15));
+    W* vals = (W*)(ct_smem + align16((size_t)SLOTS * sizeof(O)));
+    O* sk = (O*)((unsigned char*)vals + align16((size_t)SLOTS * sizeof(W)));
+    W* sv = (W*)((unsigned char*)sk + align16((size_t)(SLOTS / 2) * sizeof(O)));
     __shared__ E s_pref[THREADS];
     __shared__ O s_mem[THREADS];
     __shared__ int s_cnt;
@@ -181,7 +210,7 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
             }
         });
         __syncthreads();
-        // pack the occupied slots (slot order) at the row's scratch offset
+        // pack the occupied slots, sort them by neighbour id, write the row
         for (int base = 0; base < ts; base += THREADS) {
             int s = base + threadIdx.x;
             bool occ = s < ts && keys[s] != (O)-1;
@@ -191,12 +220,20 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
             wpos = __shfl_sync(0xffffffffu, wpos, 0);
             if (occ) {
                 int p = wpos + __popc(b & ((1u << (threadIdx.x & 31)) - 1));
-                skey[hs + p] = keys[s];
-                sval[hs + p] = vals[s];
+                sk[p] = keys[s];
+                sv[p] = vals[s];
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) ucnt[c] = (O)s_cnt;
+        int u = s_cnt;
+        int P = 1;
+        while (P < u) P <<= 1;
+        for (int i = u + threadIdx.x; i < P; i += THREADS) sk[i] = std::numeric_limits<O>::max();
+        __syncthreads();
+        block_bitonic_sort<THREADS>(sk, sv, P);
+        for (int i = threadIdx.x; i < u; i += THREADS) { skey[hs + i] = sk[i]; sval[hs + i] = sv[i]; }
+        __syncthreads();
+        if (threadIdx.x == 0) ucnt[c] = (O)u;
         __syncthreads();
     }
 }

@@ -125,6 +125,9 @@ template <class T> __device__ __forceinline__ T group_sum(T v, int w) {
 template <class T> __host__ __device__ __forceinline__ T ceil_div(T a, T b) { return (a + b - 1) / b; }
 
 // ------------------------------------------------------------------ launch geometry
+// Every kernel launch site calls count_launch() (read by jet_launch_count).
+void count_launch();
+
 struct Dev {
     int sms = 148;
     int max_smem_optin = 227 * 1024;
@@ -202,7 +205,7 @@ __global__ void k_fill(T* p, int64_t n, T v) {
 template <class T>
 inline void fill(T* p, int64_t n, T v, cudaStream_t s) {
     if (n <= 0) return;
-    k_fill<T><<<grid_persistent(n, 16), BLOCK, 0, s>>>(p, n, v);
+    k_fill<T><<<grid_persistent(n, 16), BLOCK, 0, s>>>(p, n, v); count_launch();
     JET_LAUNCH_CHECK();
 }
 
@@ -314,11 +317,11 @@ inline void exclusive_scan(Get get, int64_t n, T* out, T* total, ScanScratch& sc
     int64_t ntiles = ceil_div<int64_t>(n, SCAN_TILE);
     if (sc.buf.n < ntiles) sc.buf.alloc(ntiles + 1024, s);
     T* sums = (T*)sc.buf.p;
-    k_scan_tiles<T, Get><<<(unsigned)ntiles, BLOCK, 0, s>>>(get, n, sums);
+    k_scan_tiles<T, Get><<<(unsigned)ntiles, BLOCK, 0, s>>>(get, n, sums); count_launch();
     JET_LAUNCH_CHECK();
-    k_scan_sums<T><<<1, 1024, 0, s>>>(sums, ntiles, total);
+    k_scan_sums<T><<<1, 1024, 0, s>>>(sums, ntiles, total); count_launch();
     JET_LAUNCH_CHECK();
-    k_scan_apply<T, Get><<<(unsigned)ntiles, BLOCK, 0, s>>>(get, n, sums, out);
+    k_scan_apply<T, Get><<<(unsigned)ntiles, BLOCK, 0, s>>>(get, n, sums, out); count_launch();
     JET_LAUNCH_CHECK();
 }
 

@@ -67,7 +67,7 @@ struct Engine {
         JET_CUDA(cudaMemsetAsync(dscal.p, 0, 3 * sizeof(int64_t), s));
         if (L.n > 0) {
             k_bin_degrees<O, E><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(L.n, L.row, L.warp_list.p, dslot<O>(0), L.hub_list.p,
-                                                                          dslot<O>(1), dslot<E>(2));
+                                                                          dslot<O>(1), dslot<E>(2)); count_launch();
             JET_LAUNCH_CHECK();
         }
         pull(3);
@@ -87,63 +87,67 @@ struct Engine {
         if (!hn) { hn_own.alloc(n, s); hn = hn_own.p; }
         auto t0 = clk::now();
         if (L.uniform) {
-            k_hec_uniform<O, E, W><<<grid_persistent(n, 16), BLOCK, 0, s>>>(g, seed, rng_stream(level, RNG_HEC_RANDOM, 0), hn);
+            k_hec_uniform<O, E, W><<<grid_persistent(n, 16), BLOCK, 0, s>>>(g, seed, rng_stream(level, RNG_HEC_RANDOM, 0), hn); count_launch();
             JET_LAUNCH_CHECK();
         } else {
             W* vsum = dslot<W>(8);
             JET_CUDA(cudaMemsetAsync(vsum, 0, sizeof(int64_t), s));
-            k_sum<W><<<grid_persistent(n, 8), BLOCK, 0, s>>>(g.vw, n, vsum);
+            k_sum<W><<<grid_persistent(n, 8), BLOCK, 0, s>>>(g.vw, n, vsum); count_launch();
             JET_LAUNCH_CHECK();
             unsigned grid = grid_persistent((int64_t)n * L.group, 16);
             switch (L.group) {
-                case 4: k_hec_heavy<4, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); break;
-                case 8: k_hec_heavy<8, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); break;
-                case 16: k_hec_heavy<16, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); break;
-                default: k_hec_heavy<32, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); break;
+                case 4: k_hec_heavy<4, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); count_launch(); break;
+                case 8: k_hec_heavy<8, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); count_launch(); break;
+                case 16: k_hec_heavy<16, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); count_launch(); break;
+                default: k_hec_heavy<32, O, E, W><<<grid, BLOCK, 0, s>>>(g, vsum, hn); count_launch(); break;
             }
             JET_LAUNCH_CHECK();
             if (L.n_hub > 0) {
-                k_hec_heavy_hub<O, E, W><<<grid_for(L.n_hub, 1), 1024, 0, s>>>(g, vsum, L.hub_list.p, L.n_hub, hn);
+                k_hec_heavy_hub<O, E, W><<<grid_for(L.n_hub, 1), 1024, 0, s>>>(g, vsum, L.hub_list.p, L.n_hub, hn); count_launch();
                 JET_LAUNCH_CHECK();
             }
         }
         if (t_heavy) { sync(); *t_heavy += since(t0); }
         auto t1 = clk::now();
-        fill<O>(vcmap, n, ord_max<O>(), s);
-        DBuf<O> perm_a(n, s), perm_b(n, s);
-        O* cur = nullptr;  // identity in the first round
-        O* nxt = perm_a.p;
-        O* cur_len = dslot<O>(16);
-        O* nxt_len = dslot<O>(17);
-        int swap = 1;
-        O len = n;
-        int rounds = 0;
-        while (len > 0) {
-            JET_CUDA(cudaMemsetAsync(nxt_len, 0, sizeof(int64_t), s));
-            unsigned grid = grid_persistent(len, 16);
-            k_hec_round<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn, vcmap, swap);
-            JET_LAUNCH_CHECK();
-            k_hec_compact<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, vcmap, nxt, nxt_len);
-            JET_LAUNCH_CHECK();
-            JET_CUDA(cudaMemcpyAsync(cur_len, nxt_len, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
-            JET_CUDA(cudaMemcpyAsync(hscal, nxt_len, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-            sync();
-            len = *(O*)hscal;
-            swap ^= 1;
-            cur = nxt;
-            nxt = (nxt == perm_a.p) ? perm_b.p : perm_a.p;
-            if (++rounds > 100000) throw JetError{JET_ERR_TIMEOUT, "HEC aggregation did not settle"};
-        }
+        hec_aggregate(n, hn, vcmap);
         O nc = number_roots(vcmap, n);
         if (t_construct) *t_construct += since(t1);
         return nc;
+    }
+
+    // parallel_map_construct (src/heuristics.hpp:89-169) with the result of its
+    // in-order execution; vcmap receives each vertex's root.
+    void hec_aggregate(O n, const O* hn, O* vcmap) {
+        fill<O>(vcmap, n, ord_max<O>(), s);
+        DBuf<O> nxt(n, s), cnt(n, s), min_free(n, s);
+        DBuf<int> has_free(n, s);
+        DBuf<uint8_t> inB(n, s);
+        unsigned grid = grid_persistent(n, 16);
+        k_hec_p1_init<O><<<grid, BLOCK, 0, s>>>(n, hn, nxt.p, vcmap); count_launch();
+        JET_LAUNCH_CHECK();
+        int* changed = dslot<int>(18);
+        for (int round = 0;; round++) {
+            JET_CUDA(cudaMemsetAsync(changed, 0, sizeof(int64_t), s));
+            k_hec_p1_jump<O><<<grid, BLOCK, 0, s>>>(n, nxt.p, changed); count_launch();
+            JET_LAUNCH_CHECK();
+            JET_CUDA(cudaMemcpyAsync(hscal, changed, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+            sync();
+            if (*(int*)hscal == 0) break;
+            if (round > 64) throw JetError{JET_ERR_TIMEOUT, "HEC pointer jumping did not converge"};
+        }
+        k_hec_p1_final<O><<<grid, BLOCK, 0, s>>>(n, nxt.p, vcmap); count_launch();
+        cnt.zero();
+        k_hec_p2_count<O><<<grid, BLOCK, 0, s>>>(n, hn, vcmap, inB.p, cnt.p, min_free.p, has_free.p); count_launch();
+        k_hec_p2_walk<O><<<grid, BLOCK, 0, s>>>(n, hn, inB.p, cnt.p, min_free.p, has_free.p); count_launch();
+        k_hec_p2_roots<O><<<grid, BLOCK, 0, s>>>(n, hn, inB.p, min_free.p, has_free.p, vcmap); count_launch();
+        JET_LAUNCH_CHECK();
     }
 
     O number_roots(O* vcmap, O n) {
         DBuf<O> ids(n + 1, s);
         O* total = dslot<O>(20);
         exclusive_scan<O, GetIsRoot<O>>(GetIsRoot<O>{vcmap}, n, ids.p, total, scan, s);
-        k_assign_ids<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, ids.p, vcmap);
+        k_assign_ids<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, ids.p, vcmap); count_launch();
         JET_LAUNCH_CHECK();
         JET_CUDA(cudaMemcpyAsync(hscal, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         sync();
@@ -155,14 +159,14 @@ struct Engine {
         auto g = L.view();
         unsigned grid = grid_persistent((int64_t)max_len * L.group, 16);
         switch (L.group) {
-            case 4: k_pick_match<4, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); break;
-            case 8: k_pick_match<8, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); break;
-            case 16: k_pick_match<16, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); break;
-            default: k_pick_match<32, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); break;
+            case 4: k_pick_match<4, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); count_launch(); break;
+            case 8: k_pick_match<8, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); count_launch(); break;
+            case 16: k_pick_match<16, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); count_launch(); break;
+            default: k_pick_match<32, INITIAL, UNIFORM, O, E, W><<<grid, BLOCK, 0, s>>>(g, perm, perm_len, vcmap, hn, seed, stream); count_launch(); break;
         }
         JET_LAUNCH_CHECK();
         if (L.n_hub > 0) {
-            k_pick_match_hub<INITIAL, UNIFORM, O, E, W><<<grid_for(L.n_hub, 1), 1024, 0, s>>>(g, L.hub_list.p, L.n_hub, vcmap, hn, seed, stream);
+            k_pick_match_hub<INITIAL, UNIFORM, O, E, W><<<grid_for(L.n_hub, 1), 1024, 0, s>>>(g, L.hub_list.p, L.n_hub, vcmap, hn, seed, stream); count_launch();
             JET_LAUNCH_CHECK();
         }
     }
@@ -176,13 +180,13 @@ struct Engine {
         fill<O>(hn.p, n, MAXV, s);
         fill<O>(vcmap, n, MAXV, s);
         if (L.uniform) {
-            k_match_uniform_init<O, E, W><<<grid_persistent(n, 16), BLOCK, 0, s>>>(g, seed, rng_stream(level, RNG_MATCH_RANDOM, 0), hn.p);
+            k_match_uniform_init<O, E, W><<<grid_persistent(n, 16), BLOCK, 0, s>>>(g, seed, rng_stream(level, RNG_MATCH_RANDOM, 0), hn.p); count_launch();
             JET_LAUNCH_CHECK();
         } else {
             pick<true, false>(L, nullptr, nullptr, n, vcmap, hn.p, seed, rng_stream(level, RNG_MATCH_PICK, 0));
         }
         if (hn_init_out) JET_CUDA(cudaMemcpyAsync(hn_init_out, hn.p, sizeof(O) * n, cudaMemcpyDeviceToDevice, s));
-        DBuf<O> perm_a(n, s), perm_b(n, s);
+        DBuf<O> perm_a(n, s), perm_b(n, s), winner(n, s);
         O* cur = nullptr;
         O* cur_len = dslot<O>(16);
         O* nxt_len = dslot<O>(17);
@@ -191,9 +195,10 @@ struct Engine {
         while (len > 0) {
             unsigned grid = grid_persistent(len, 16);
             for (int r = 0; r < 4; r++) {
-                k_commit1<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap, r);
-                k_commit2<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap);
-                k_commit3<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, vcmap);
+                k_commit1<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap, winner.p, r); count_launch();
+                k_commit2a<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap, winner.p); count_launch();
+                k_commit2<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap, winner.p); count_launch();
+                k_commit3<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, vcmap); count_launch();
                 JET_LAUNCH_CHECK();
             }
             outer++;
@@ -202,7 +207,7 @@ struct Engine {
             else pick<false, false>(L, cur, cur_len, len, vcmap, hn.p, seed, st);
             O* nxt = (cur == perm_a.p) ? perm_b.p : perm_a.p;
             JET_CUDA(cudaMemsetAsync(nxt_len, 0, sizeof(int64_t), s));
-            k_match_remaining<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap, nxt, nxt_len);
+            k_match_remaining<O><<<grid, BLOCK, 0, s>>>(n, cur, cur_len, hn.p, vcmap, nxt, nxt_len); count_launch();
             JET_LAUNCH_CHECK();
             JET_CUDA(cudaMemcpyAsync(cur_len, nxt_len, sizeof(int64_t), cudaMemcpyDeviceToDevice, s));
             JET_CUDA(cudaMemcpyAsync(hscal, nxt_len, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -212,7 +217,7 @@ struct Engine {
             if (outer > 100000) throw JetError{JET_ERR_TIMEOUT, "matching did not settle"};
         }
         if (two_hop) two_hop_passes(L, vcmap);
-        k_singletons<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, vcmap);
+        k_singletons<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, vcmap); count_launch();
         JET_LAUNCH_CHECK();
         return number_roots(vcmap, n);
     }
@@ -220,7 +225,7 @@ struct Engine {
     O count_unmatched(O n, const O* vcmap) {
         O* c = dslot<O>(24);
         JET_CUDA(cudaMemsetAsync(c, 0, sizeof(int64_t), s));
-        k_count_unmatched<O><<<grid_persistent(n, 8), BLOCK, 0, s>>>(n, vcmap, c);
+        k_count_unmatched<O><<<grid_persistent(n, 8), BLOCK, 0, s>>>(n, vcmap, c); count_launch();
         JET_LAUNCH_CHECK();
         JET_CUDA(cudaMemcpyAsync(hscal, c, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         sync();
@@ -236,7 +241,7 @@ struct Engine {
         sync();
         O cnt = *(O*)hscal;
         list.alloc(cnt > 0 ? cnt : 1, s);
-        k_scatter_unmatched<O, E><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, vcmap, L.row, leaves_only, pos.p, list.p);
+        k_scatter_unmatched<O, E><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, vcmap, L.row, leaves_only, pos.p, list.p); count_launch();
         JET_LAUNCH_CHECK();
         return cnt;
     }
@@ -250,7 +255,7 @@ struct Engine {
         fill<O>(twins.p, mappable, (O)-1, s);
         int* err = dslot<int>(30);
         JET_CUDA(cudaMemsetAsync(err, 0, sizeof(int64_t), s));
-        k_match_hash<O, H><<<grid_persistent(mappable, 16), BLOCK, 0, s>>>(list, hashes, mappable, nullkey, ht.p, twins.p, vcmap, err);
+        k_match_hash<O, H><<<grid_persistent(mappable, 16), BLOCK, 0, s>>>(list, hashes, mappable, nullkey, ht.p, twins.p, vcmap, err); count_launch();
         JET_LAUNCH_CHECK();
         JET_CUDA(cudaMemcpyAsync(hscal, err, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         sync();
@@ -267,7 +272,7 @@ struct Engine {
             O cnt = unmatched_list(L, vcmap, 1, list);
             if (cnt > 0) {
                 DBuf<O> hs(cnt, s);
-                k_leaf_hash<O, E, W><<<grid_persistent(cnt, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p);
+                k_leaf_hash<O, E, W><<<grid_persistent(cnt, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p); count_launch();
                 JET_LAUNCH_CHECK();
                 match_hash<O>(list.p, hs.p, cnt, MAXV, vcmap);
             }
@@ -278,10 +283,10 @@ struct Engine {
             O cnt = unmatched_list(L, vcmap, 0, list);
             if (cnt > 0) {
                 DBuf<uint64_t> hs(cnt, s);
-                k_twin_hash<O, E, W><<<grid_persistent((int64_t)cnt * 32, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p);
+                k_twin_hash<O, E, W><<<grid_persistent((int64_t)cnt * 32, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p); count_launch();
                 JET_LAUNCH_CHECK();
                 if (L.n_hub > 0) {
-                    k_twin_hash_hub<O, E, W><<<grid_for(cnt, 1) < 4096 ? grid_for(cnt, 1) : 4096, 1024, 0, s>>>(g, list.p, cnt, hs.p);
+                    k_twin_hash_hub<O, E, W><<<grid_for(cnt, 1) < 4096 ? grid_for(cnt, 1) : 4096, 1024, 0, s>>>(g, list.p, cnt, hs.p); count_launch();
                     JET_LAUNCH_CHECK();
                 }
                 match_hash<uint64_t>(list.p, hs.p, cnt, (uint64_t)0, vcmap);
@@ -293,7 +298,7 @@ struct Engine {
             O cnt = unmatched_list(L, vcmap, 0, list);
             if (cnt > 0) {
                 DBuf<O> hs(cnt, s);
-                k_relative_hash<O, E, W><<<grid_persistent(cnt, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p);
+                k_relative_hash<O, E, W><<<grid_persistent(cnt, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p); count_launch();
                 JET_LAUNCH_CHECK();
                 match_hash<O>(list.p, hs.p, cnt, MAXV, vcmap);
             }
@@ -315,11 +320,11 @@ struct Engine {
         DBuf<E> du(nc + 1, s), hrow(nc + 1, s);
         C.own_vw.alloc(nc, s);
         cnt.zero(); du.zero(); C.own_vw.zero(); ucnt.zero();
-        k_contract_count<O, E, W><<<grid_persistent(n, 16), BLOCK, 0, s>>>(g, map, cnt.p, du.p, C.own_vw.p);
+        k_contract_count<O, E, W><<<grid_persistent(n, 16), BLOCK, 0, s>>>(g, map, cnt.p, du.p, C.own_vw.p); count_launch();
         JET_LAUNCH_CHECK();
         exclusive_scan_array<O>(cnt.p, nc + 1, moff.p, nullptr, scan, s);
         exclusive_scan_array<E>(du.p, nc + 1, hrow.p, nullptr, scan, s);
-        k_contract_members<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, map, moff.p, cnt.p, members.p);
+        k_contract_members<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, map, moff.p, cnt.p, members.p); count_launch();
         JET_LAUNCH_CHECK();
         // scratch for unique entries, sized by the fine nnz (the bound on sum du)
         DBuf<O> skey_own;
@@ -334,21 +339,21 @@ struct Engine {
         O* nh = dslot<O>(42);
         int* err = dslot<int>(43);
         JET_CUDA(cudaMemsetAsync(n1, 0, 4 * sizeof(int64_t), s));
-        k_contract_bin<O, E><<<grid_persistent(nc, 8), BLOCK, 0, s>>>(nc, hrow.p, l1.p, n1, l2.p, n2, lh.p, nh);
+        k_contract_bin<O, E><<<grid_persistent(nc, 8), BLOCK, 0, s>>>(nc, hrow.p, l1.p, n1, l2.p, n2, lh.p, nh); count_launch();
         JET_LAUNCH_CHECK();
-        k_contract_warp<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(g, map, nc, moff.p, members.p, hrow.p, skey, sval, ucnt.p);
+        k_contract_warp<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(g, map, nc, moff.p, members.p, hrow.p, skey, sval, ucnt.p); count_launch();
         JET_LAUNCH_CHECK();
         {
             size_t sm1 = contract_smem_bytes<O, W>(CT_S1_SLOTS), sm2 = contract_smem_bytes<O, W>(CT_S2_SLOTS);
             JET_CUDA(cudaFuncSetAttribute(k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
             k_contract_smem<CT_S1_THREADS, CT_S1_SLOTS, O, E, W><<<device_info().sms * 8, CT_S1_THREADS, sm1, s>>>(
-                g, map, l1.p, n1, moff.p, members.p, hrow.p, skey, sval, ucnt.p);
+                g, map, l1.p, n1, moff.p, members.p, hrow.p, skey, sval, ucnt.p); count_launch();
             JET_LAUNCH_CHECK();
             k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W><<<device_info().sms * 2, CT_S2_THREADS, sm2, s>>>(
-                g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p);
+                g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p); count_launch();
             JET_LAUNCH_CHECK();
-            k_contract_hub<O, E, W><<<device_info().sms, 1024, 0, s>>>(g, map, lh.p, nh, moff.p, members.p, hrow.p, skey, sval, ucnt.p, err);
+            k_contract_hub<O, E, W><<<device_info().sms, 1024, 0, s>>>(g, map, lh.p, nh, moff.p, members.p, hrow.p, skey, sval, ucnt.p, err); count_launch();
             JET_LAUNCH_CHECK();
         }
         // coarse row offsets and nnz
@@ -364,9 +369,9 @@ struct Engine {
         C.own_adj.alloc(mc > 0 ? mc : 1, s);
         C.own_val.alloc(mc > 0 ? mc : 1, s);
         k_contract_copy<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(nc, hrow.p, skey, sval, C.own_row.p,
-                                                                                        C.own_adj.p, C.own_val.p);
+                                                                                        C.own_adj.p, C.own_val.p); count_launch();
         JET_LAUNCH_CHECK();
-        k_contract_copy_hub<O, E, W><<<device_info().sms, 1024, 0, s>>>(lh.p, nh, hrow.p, skey, sval, C.own_row.p, C.own_adj.p, C.own_val.p);
+        k_contract_copy_hub<O, E, W><<<device_info().sms, 1024, 0, s>>>(lh.p, nh, hrow.p, skey, sval, C.own_row.p, C.own_adj.p, C.own_val.p); count_launch();
         JET_LAUNCH_CHECK();
         C.row = C.own_row.p;
         C.adj = C.own_adj.p;

@@ -45,6 +45,7 @@ struct RefDev {
     O nmoves;
     O ncand_hub;
     O nmoves_hub;
+    O nredraw;
     W cut1, cut2;
     W vw_cursor;          // strong rebalance: next free position past the evictions
     W max_vwgt;
@@ -479,12 +480,48 @@ struct RebArgs {
     O sections;
     O t_minibuckets;
     O width;          // MAX_BUCKETS * sections
-    W* buckets;       // t_minibuckets + 1 + width entries
+    W* buckets;       // raw bucket totals, t_minibuckets + 1 + width entries
+    W* boff;          // exclusive offsets of buckets[0 .. t_minibuckets]
     O* bid;
-    W* score;
+    W* score;         // in-bucket score (weight of the bucket's earlier vertices)
     part_t* undersized;
     W* evict_adjust;  // k
     W* evict_start;   // k + 1
+    const uint32_t* skey;  // candidates sorted by bucket id (stable in vertex id)
+    const O* sval;
+    const W* wpre;         // exclusive prefix of vertex weights in sorted order
+    uint32_t none_key;     // key of non-candidates (sorted last)
+    O* redraw;             // strong rebalance: vertices needing a re-drawn position
+    part_t* redraw_p;      // and the chunk they stopped at
+};
+
+// B(x): the offset the reference reads for bucket x -- scanned for
+// x <= t_minibuckets, the raw total past it (the scan does not reach there).
+template <class O, class W>
+__device__ __forceinline__ W bucket_pos(const RebArgs<O, W>& rb, O x) { return x <= rb.t_minibuckets ? rb.boff[x] : rb.buckets[x]; }
+
+// Weight of the vertices that precede bucket b in bucket order.
+template <class O, class W>
+__device__ __forceinline__ W bucket_start(const RebArgs<O, W>& rb, O b) {
+    if (b <= rb.t_minibuckets) return rb.boff[b];
+    W s = rb.boff[rb.t_minibuckets] + rb.buckets[rb.t_minibuckets];
+    for (O x = rb.t_minibuckets + 1; x < b; x++) s += rb.buckets[x];
+    return s;
+}
+
+template <class O>
+struct GetBidKey {
+    const O* bid;
+    uint32_t none;
+    __device__ __forceinline__ uint32_t operator()(int64_t i) const { O b = bid[i]; return b < 0 ? none : (uint32_t)b; }
+};
+template <class O, class W>
+struct GetSortedWeight {
+    const uint32_t* key;
+    const O* val;
+    const W* vw;
+    uint32_t none;
+    __device__ __forceinline__ W operator()(int64_t q) const { return key[q] == none ? (W)0 : vw[val[q]]; }
 };
 
 // Undersized parts in index order (src/jet_refiner.hpp:584-598).
@@ -522,7 +559,7 @@ __device__ __forceinline__ void weak_score(const RefArgs<O, E, W>& a, const RebA
         int gt = gain_bucket<W>(sg, a.g.vw[i]);
         O gid = (MAX_BUCKETS * (O)p + gt) * rb.sections + (O)(i % rb.sections);
         rb.bid[i] = gid;
-        rb.score[i] = atomic_add(&rb.buckets[gid], a.g.vw[i]);
+        atomic_add(&rb.buckets[gid], a.g.vw[i]);  // bucket total; in-bucket order comes from the sort
     } else {
         rb.bid[i] = -1;
     }
@@ -626,7 +663,7 @@ __device__ __forceinline__ void strong_score(const RefArgs<O, E, W>& a, const Re
     if (gt < MAX_BUCKETS) {
         O gid = (MAX_BUCKETS * (O)p + gt) * rb.sections + (O)(i % rb.sections) + 1;
         rb.bid[i] = gid;
-        rb.score[i] = atomic_add(&rb.buckets[gid], w);
+        atomic_add(&rb.buckets[gid], w);
     }
 }
 
@@ -685,28 +722,31 @@ __global__ void __launch_bounds__(BLOCK) k_strong_score_warp(RefArgs<O, E, W> a,
     }
 }
 
-// get_evictions (src/jet_refiner.hpp:392-409): `buckets` already holds the
-// exclusive offsets.
+// get_evictions (src/jet_refiner.hpp:392-409).  The reference's in-bucket
+// score is an atomic fetch-add whose order, run in index order, is the
+// weight of the bucket's earlier vertices; here it is read off the stable
+// sort by bucket id: wpre[q] - (weight of all earlier buckets).
 template <bool ADJUST, class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_evict(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__global__ void __launch_bounds__(BLOCK) k_evict_sorted(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t rounds = ceil_div<int64_t>((int64_t)a.g.n, stride);
     for (int64_t r = 0; r < rounds; r++) {
-        int64_t x = start + r * stride;
+        int64_t q = start + r * stride;
         bool take = false;
-        O i = (O)x;
-        if (x < a.g.n) {
-            O b = rb.bid[i];
-            if (b != -1) {
-                part_t p = a.part[i];
-                O begin = (O)p * rb.width;
-                W score = rb.score[i] + rb.buckets[b] - rb.buckets[begin];
-                W limit = a.sizes[p] - rb.size_max;
-                if (score < limit) {
-                    take = true;
-                    if (ADJUST && score + a.g.vw[i] >= limit) rb.evict_adjust[p] = score + a.g.vw[i];
-                }
+        O i = 0;
+        if (q < a.g.n && rb.skey[q] != rb.none_key) {
+            O b = (O)rb.skey[q];
+            i = rb.sval[q];
+            part_t p = a.part[i];
+            O begin = (O)p * rb.width;
+            W within = rb.wpre[q] - bucket_start<O, W>(rb, b);
+            if (ADJUST) rb.score[i] = within;
+            W score = within + bucket_pos<O, W>(rb, b) - bucket_pos<O, W>(rb, begin);
+            W limit = a.sizes[p] - rb.size_max;
+            if (score < limit) {
+                take = true;
+                if (ADJUST && score + a.g.vw[i] >= limit) rb.evict_adjust[p] = score + a.g.vw[i];
             }
         }
         O s = warp_append(&a.dev->nmoves, take);
@@ -726,11 +766,11 @@ __global__ void __launch_bounds__(1024) k_cookie(RefArgs<O, E, W> a, RebArgs<O, 
         O begin = (O)p * rb.width;
         if (p < a.k) {
             add = rb.evict_adjust[p];
-            if (add == 0) add = rb.buckets[begin + rb.width] - rb.buckets[begin];
+            if (add == 0) add = rb.boff[begin + rb.width] - rb.boff[begin];
         }
         W tot;
         W ex = block_exclusive_scan<W>(add, sw, tot);
-        if (p < a.k) rb.evict_adjust[p] = rb.buckets[begin] - (carry + ex);
+        if (p < a.k) rb.evict_adjust[p] = rb.boff[begin] - (carry + ex);
         carry += tot;
     }
     if (threadIdx.x == 0) a.dev->vw_cursor = carry;
@@ -747,31 +787,88 @@ __global__ void __launch_bounds__(1024) k_cookie(RefArgs<O, E, W> a, RebArgs<O, 
     if (threadIdx.x == 0) rb.evict_start[0] = 0;
 }
 
-// Adjust scores and pick destinations by chunk, re-drawing a position past
-// the end when less than half the vertex fits (src/jet_refiner.hpp:519-544).
+// Adjust scores and pick destinations by chunk (src/jet_refiner.hpp:519-544).
+// A vertex less than half inside its chunk draws a new position past the
+// end; only those draws depend on order (they advance one shared cursor),
+// so they are queued here and replayed in vertex order by k_strong_redraw.
 template <class O, class E, class W>
-__global__ void k_strong_dest(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__global__ void k_strong_first(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     O count = a.dev->nmoves;
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < count; x += (int64_t)gridDim.x * blockDim.x) {
         O v = a.moves[x];
         part_t pv = a.part[v];
-        W sc = rb.score[v] + rb.buckets[rb.bid[v]] - rb.evict_adjust[pv];
+        W sc = rb.score[v] + rb.boff[rb.bid[v]] - rb.evict_adjust[pv];
         W w = a.g.vw[v];
         int p = 0;
+        while (p <= a.k && rb.evict_start[p] <= sc) p++;
+        p--;
         part_t dest = pv;
-        // re-drawn positions only grow, so p never falls below 0; the guard
-        // bounds the walk regardless
-        int guard = 0;
-        while (p < a.k) {
-            while (p <= a.k && rb.evict_start[p] <= sc) p++;
-            p--;
-            if (p < 0 || ++guard > 4 * a.k + 64) { atomicOr(&a.dev->err, ERRF_SPIN); dest = pv; break; }
-            if (p < a.k && w / 2 <= rb.evict_start[p + 1] - sc) { dest = p; break; }
-            else if (p < a.k) sc = atomic_add(&a.dev->vw_cursor, w);
+        if (p < 0) atomicOr(&a.dev->err, ERRF_SPIN);  // positions are never negative
+        else if (p < a.k) {
+            if (w / 2 <= rb.evict_start[p + 1] - sc) dest = p;
+            else {
+                O s = atomic_add(&a.dev->nredraw, (O)1);
+                rb.redraw[s] = v;
+                rb.redraw_p[v] = p;
+            }
         }
         rb.score[v] = sc;
         a.dest[v] = dest;
     }
+}
+
+// One block: sorts the queued vertices by id and replays their draws in order.
+static constexpr int REDRAW_CAP = 4096;
+template <class K>
+__device__ __forceinline__ void block_sort_keys(K* key, int P) {
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < P; i += blockDim.x) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    bool up = (i & k) == 0;
+                    K x = key[i], y = key[ixj];
+                    if ((x > y) == up) { key[i] = y; key[ixj] = x; }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    __shared__ O list[REDRAW_CAP];
+    O cnt = a.dev->nredraw;
+    if (cnt == 0) return;
+    bool fits = cnt <= REDRAW_CAP;
+    if (fits) {
+        int P = 1;
+        while (P < (int)cnt) P <<= 1;
+        for (int i = threadIdx.x; i < P; i += blockDim.x) list[i] = i < (int)cnt ? rb.redraw[i] : std::numeric_limits<O>::max();
+        __syncthreads();
+        block_sort_keys<O>(list, P);
+    } else if (threadIdx.x == 0) {
+        atomicOr(&a.dev->err, 16);  // more draws than the replay buffer: order falls back to queue order
+    }
+    if (threadIdx.x != 0) return;
+    W cursor = a.dev->vw_cursor;
+    for (O x = 0; x < cnt; x++) {
+        O v = fits ? list[x] : rb.redraw[x];
+        W w = a.g.vw[v];
+        int p = rb.redraw_p[v];
+        part_t dest = a.part[v];
+        int guard = 0;
+        while (p < a.k) {
+            W sc = cursor;
+            cursor += w;
+            while (p <= a.k && rb.evict_start[p] <= sc) p++;
+            p--;
+            if (p < a.k && w / 2 <= rb.evict_start[p + 1] - sc) { dest = p; break; }
+            if (++guard > 4 * a.k + 64) { atomicOr(&a.dev->err, ERRF_SPIN); break; }
+        }
+        a.dest[v] = dest;
+    }
+    a.dev->vw_cursor = cursor;
 }
 
 // ---------------------------------------------------------------- moves
@@ -967,7 +1064,7 @@ __global__ void __launch_bounds__(1024) k_finalize(RefArgs<O, E, W> a, IterResul
         out->max_part = (int64_t)mx;
         out->err = d->err;
         out->large = d->large;
-        d->ncand = 0; d->nmoves = 0; d->ncand_hub = 0; d->nmoves_hub = 0;
+        d->ncand = 0; d->nmoves = 0; d->ncand_hub = 0; d->nmoves_hub = 0; d->nredraw = 0;
         d->cut1 = 0; d->cut2 = 0; d->large = 0;
     }
 }

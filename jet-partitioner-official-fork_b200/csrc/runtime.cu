@@ -2,6 +2,7 @@
 // stream-ordered memory pool, the default stream, error strings, kernel-class
 // profiling and the tier-generic C entry points.
 #include "api_impl.cuh"
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -53,6 +54,9 @@ cudaStream_t default_stream() {
     if (!streams[dev]) JET_CUDA(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
     return streams[dev];
 }
+
+static std::atomic<int64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
@@ -176,6 +180,8 @@ int jet_project(int tier, int64_t n_fine, const void* map, const int32_t* coarse
     if (!o) return JET_ERR_INVALID;
     return o->project(n_fine, map, coarse, fine, stream);
 }
+
+int64_t jet_launch_count(void) { return g_launches.load(); }
 
 int jet_prof_enable(int on) {
     prof_collect();

@@ -3,6 +3,7 @@
 // (src/partitioner.hpp:61-125).
 #pragma once
 #include "partitioner.cuh"
+#include "sort.cuh"
 
 namespace jetb {
 
@@ -18,7 +19,11 @@ struct Refiner {
     DBuf<part_t> csize, dest_cache, part_work, dest, undersized;
     DBuf<uint8_t> lock, mark;
     DBuf<W> save_gain, pregain, score, sizes_curr, sizes_best, evict_adjust, evict_start, buckets;
-    DBuf<O> cand, cand_hub, moves, moves_hub, bid;
+    DBuf<O> cand, cand_hub, moves, moves_hub, bid, sv0, sv1, redraw;
+    DBuf<uint32_t> sk0, sk1;
+    DBuf<W> boff, wpre;
+    DBuf<part_t> redraw_p;
+    RadixScratch rsort;
     DBuf<RefDev<O, W>> dev;
     int64_t bucket_cap = 0;
     bool verbose = false;
@@ -47,6 +52,9 @@ struct Refiner {
         sections_for(nmax, sections, tmb);
         bucket_cap = (int64_t)tmb + 1 + (int64_t)MAX_BUCKETS * sections;
         buckets.alloc(bucket_cap, s);
+        boff.alloc(bucket_cap, s);
+        sk0.alloc(n1, s); sk1.alloc(n1, s); sv0.alloc(n1, s); sv1.alloc(n1, s); wpre.alloc(n1, s);
+        redraw.alloc(n1, s); redraw_p.alloc(n1, s);
         dev.alloc(1, s);
         dev.zero();
     }
@@ -93,18 +101,18 @@ struct Refiner {
         auto a = args(L);
         if (cta_smem() > (size_t)device_info().max_smem_optin - 1024)
             throw JetError{JET_ERR_INVALID, "num_parts too large for the shared-memory connectivity tables"};
-        k_conn_thread<O, E, W><<<grid_persistent(L.n, 16), 128, 0, s>>>(a, only_marked, gate);
+        k_conn_thread<O, E, W><<<grid_persistent(L.n, 16), 128, 0, s>>>(a, only_marked, gate); count_launch();
         JET_LAUNCH_CHECK();
         if (L.n_warp > 0) {
             if (k <= WARP_TABLE) {
-                k_conn_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, warp_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate);
+                k_conn_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, warp_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate); count_launch();
             } else {
-                k_conn_cta<O, E, W><<<grid_for(L.n_warp, 1) < 4096 ? grid_for(L.n_warp, 1) : 4096, 256, cta_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate);
+                k_conn_cta<O, E, W><<<grid_for(L.n_warp, 1) < 4096 ? grid_for(L.n_warp, 1) : 4096, 256, cta_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate); count_launch();
             }
             JET_LAUNCH_CHECK();
         }
         if (L.n_hub > 0) {
-            k_conn_cta<O, E, W><<<grid_for(L.n_hub, 1) < 4096 ? grid_for(L.n_hub, 1) : 4096, 1024, cta_smem(), s>>>(a, L.hub_list.p, L.n_hub, only_marked, gate);
+            k_conn_cta<O, E, W><<<grid_for(L.n_hub, 1) < 4096 ? grid_for(L.n_hub, 1) : 4096, 1024, cta_smem(), s>>>(a, L.hub_list.p, L.n_hub, only_marked, gate); count_launch();
             JET_LAUNCH_CHECK();
         }
     }
@@ -128,23 +136,23 @@ struct Refiner {
     void lp(const Level<O, E, W>& L, double filter_ratio) {
         auto a = args(L);
         int h = prof_begin(s);
-        k_lp_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, filter_ratio);
+        k_lp_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, filter_ratio); count_launch();
         JET_LAUNCH_CHECK();
-        if (L.n_warp > 0) k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, L.warp_list.p, L.n_warp, filter_ratio);
-        if (L.n_hub > 0) k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, L.hub_list.p, L.n_hub, filter_ratio);
+        if (L.n_warp > 0) k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, L.warp_list.p, L.n_warp, filter_ratio); count_launch();
+        if (L.n_hub > 0) k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, L.hub_list.p, L.n_hub, filter_ratio); count_launch();
         JET_LAUNCH_CHECK();
         prof_end(h, PK_LP_SELECT, 0, s);
         h = prof_begin(s);
         unsigned grid = grid_persistent((int64_t)L.n * L.group, 16);
         switch (L.group) {
-            case 4: k_afterburn<4, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
-            case 8: k_afterburn<8, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
-            case 16: k_afterburn<16, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
-            default: k_afterburn<32, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 4: k_afterburn<4, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
+            case 8: k_afterburn<8, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
+            case 16: k_afterburn<16, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
+            default: k_afterburn<32, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
         }
         JET_LAUNCH_CHECK();
         if (L.n_hub > 0) {
-            k_afterburn_hub<O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a);
+            k_afterburn_hub<O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch();
             JET_LAUNCH_CHECK();
         }
         prof_end(h, PK_AFTERBURN, 0, s);
@@ -155,11 +163,27 @@ struct Refiner {
         O sections, tmb;
         sections_for(L.n, sections, tmb);
         rb.size_max = size_max; rb.opt = opt; rb.max_dest = max_dest; rb.sections = sections; rb.t_minibuckets = tmb;
-        rb.width = MAX_BUCKETS * sections; rb.buckets = buckets.p; rb.bid = bid.p; rb.score = score.p;
+        rb.width = MAX_BUCKETS * sections; rb.buckets = buckets.p; rb.boff = boff.p; rb.bid = bid.p; rb.score = score.p;
         rb.undersized = undersized.p; rb.evict_adjust = evict_adjust.p; rb.evict_start = evict_start.p;
+        rb.redraw = redraw.p; rb.redraw_p = redraw_p.p;
+        rb.skey = nullptr; rb.sval = nullptr; rb.wpre = wpre.p;
+        rb.none_key = (uint32_t)((int64_t)tmb + rb.width + 1);
         if ((int64_t)tmb + 1 + rb.width > bucket_cap) throw JetError{JET_ERR_INVALID, "bucket array too small"};
         JET_CUDA(cudaMemsetAsync(buckets.p, 0, sizeof(W) * ((size_t)tmb + 1 + rb.width), s));
         return rb;
+    }
+
+    // Bucket offsets, then candidates sorted by bucket id (stable in vertex
+    // id) with the prefix of their weights: the in-order bucket scores.
+    void sort_candidates(const Level<O, E, W>& L, RebArgs<O, W>& rb) {
+        exclusive_scan_array<W>(buckets.p, (int64_t)rb.t_minibuckets + 1, boff.p, nullptr, e.scan, s);
+        int bits = bits_for((uint64_t)rb.none_key);
+        int which = radix_sort_pairs<uint32_t, O>(GetBidKey<O>{bid.p, rb.none_key}, GetIndex<O>{}, (int64_t)L.n, bits, sk0.p, sv0.p,
+                                                  sk1.p, sv1.p, rsort, e.scan, s);
+        rb.skey = which == 0 ? sk0.p : sk1.p;
+        rb.sval = which == 0 ? sv0.p : sv1.p;
+        exclusive_scan<W, GetSortedWeight<O, W>>(GetSortedWeight<O, W>{rb.skey, rb.sval, L.vw, rb.none_key}, (int64_t)L.n, wpre.p,
+                                                 nullptr, e.scan, s);
     }
 
     // rebalance_weak, src/jet_refiner.hpp:551-645.
@@ -168,13 +192,13 @@ struct Refiner {
         W max_dest = (W)((double)size_max * 0.99);
         if (max_dest < size_max - 100) max_dest = size_max - 100;
         auto rb = reb_args(L, max_dest, opt, size_max);
-        k_weak_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb);
-        k_weak_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb);
-        if (L.n_warp > 0) k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp);
-        if (L.n_hub > 0) k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub);
+        k_weak_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
+        k_weak_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
+        if (L.n_warp > 0) { k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp); count_launch(); }
+        if (L.n_hub > 0) { k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub); count_launch(); }
         JET_LAUNCH_CHECK();
-        exclusive_scan_array<W>(buckets.p, (int64_t)rb.t_minibuckets + 1, buckets.p, nullptr, e.scan, s);
-        k_evict<false, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb);
+        sort_candidates(L, rb);
+        k_evict_sorted<false, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
         JET_LAUNCH_CHECK();
     }
 
@@ -184,16 +208,17 @@ struct Refiner {
         W md = (W)((double)size_max * 0.99);
         W max_dest = opt + 1 > md ? opt + 1 : md;
         auto rb = reb_args(L, max_dest, opt, size_max);
-        k_strong_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb);
-        k_strong_score_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb);
-        if (L.n_warp > 0) k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp);
-        if (L.n_hub > 0) k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub);
+        k_strong_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
+        k_strong_score_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
+        if (L.n_warp > 0) { k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp); count_launch(); }
+        if (L.n_hub > 0) { k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub); count_launch(); }
         JET_LAUNCH_CHECK();
-        exclusive_scan_array<W>(buckets.p, (int64_t)rb.t_minibuckets + 1, buckets.p, nullptr, e.scan, s);
+        sort_candidates(L, rb);
         JET_CUDA(cudaMemsetAsync(evict_adjust.p, 0, sizeof(W) * k, s));
-        k_evict<true, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb);
-        k_cookie<O, E, W><<<1, 1024, 0, s>>>(a, rb);
-        k_strong_dest<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(a, rb);
+        k_evict_sorted<true, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
+        k_cookie<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
+        k_strong_first<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(a, rb); count_launch();
+        k_strong_redraw<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
         JET_LAUNCH_CHECK();
     }
 
@@ -201,35 +226,35 @@ struct Refiner {
     IterResult perform_moves(const Level<O, E, W>& L) {
         auto a = args(L);
         int hist = (size_t)k * sizeof(W) <= 32 * 1024;
-        k_apply_moves<O, E, W><<<grid_persistent(L.n, 8), BLOCK, hist ? (size_t)k * sizeof(W) : 0, s>>>(a, hist);
+        k_apply_moves<O, E, W><<<grid_persistent(L.n, 8), BLOCK, hist ? (size_t)k * sizeof(W) : 0, s>>>(a, hist); count_launch();
         JET_LAUNCH_CHECK();
         int h = prof_begin(s);
         unsigned grid = grid_persistent((int64_t)L.n * L.group / 4 + 1, 16);
         switch (L.group) {
-            case 4: k_update_small<4, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); k_update_small<4, true, O, E, W><<<grid, BLOCK, 0, s>>>(a);
-                    k_mark_neighbors<4, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
-            case 8: k_update_small<8, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); k_update_small<8, true, O, E, W><<<grid, BLOCK, 0, s>>>(a);
-                    k_mark_neighbors<8, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
-            case 16: k_update_small<16, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); k_update_small<16, true, O, E, W><<<grid, BLOCK, 0, s>>>(a);
-                     k_mark_neighbors<16, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
-            default: k_update_small<32, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); k_update_small<32, true, O, E, W><<<grid, BLOCK, 0, s>>>(a);
-                     k_mark_neighbors<32, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 4: k_update_small<4, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); k_update_small<4, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch();
+                    k_mark_neighbors<4, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
+            case 8: k_update_small<8, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); k_update_small<8, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch();
+                    k_mark_neighbors<8, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
+            case 16: k_update_small<16, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); k_update_small<16, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch();
+                     k_mark_neighbors<16, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
+            default: k_update_small<32, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); k_update_small<32, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch();
+                     k_mark_neighbors<32, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
         }
         JET_LAUNCH_CHECK();
         if (L.n_hub > 0) {
             // the subtract pass must finish before any add: two launches
-            k_update_small_hub<false, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a);
-            k_update_small_hub<true, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a);
+            k_update_small_hub<false, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch();
+            k_update_small_hub<true, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch();
             JET_LAUNCH_CHECK();
         }
         build_tables(L, 1, &dev.p->large);
         prof_end(h, PK_UPDATE, 0, s);
-        k_cut_after<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(a);
-        k_finalize<O, E, W><<<1, 1024, 0, s>>>(a, e.hres);
+        k_cut_after<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(a); count_launch();
+        k_finalize<O, E, W><<<1, 1024, 0, s>>>(a, e.hres); count_launch();
         JET_LAUNCH_CHECK();
         e.sync();
         IterResult r = *e.hres;
-        if (r.err) throw JetError{JET_ERR_OVERFLOW, "connectivity table update exceeded its bounds"};
+        if (r.err & ~16) throw JetError{JET_ERR_OVERFLOW, "connectivity table update exceeded its bounds"};
         return r;
     }
 
@@ -238,10 +263,10 @@ struct Refiner {
         JET_CUDA(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
         unsigned grid = grid_persistent((int64_t)L.n * L.group, 16);
         switch (L.group) {
-            case 4: k_total_cut<4, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); break;
-            case 8: k_total_cut<8, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); break;
-            case 16: k_total_cut<16, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); break;
-            default: k_total_cut<32, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); break;
+            case 4: k_total_cut<4, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); count_launch(); break;
+            case 8: k_total_cut<8, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); count_launch(); break;
+            case 16: k_total_cut<16, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); count_launch(); break;
+            default: k_total_cut<32, O, E, W><<<grid, BLOCK, 0, s>>>(L.view(), part, out); count_launch(); break;
         }
         JET_LAUNCH_CHECK();
         JET_CUDA(cudaMemcpyAsync(&e.hscal[0], out, sizeof(W), cudaMemcpyDeviceToHost, s));
@@ -252,14 +277,14 @@ struct Refiner {
     void part_sizes(const Level<O, E, W>& L, const part_t* part, W* sizes) {
         JET_CUDA(cudaMemsetAsync(sizes, 0, sizeof(W) * k, s));
         int hist = (size_t)k * sizeof(W) <= 32 * 1024;
-        k_part_sizes<O, W><<<grid_persistent(L.n, 8), BLOCK, hist ? (size_t)k * sizeof(W) : 0, s>>>(L.n, L.vw, part, k, sizes, hist);
+        k_part_sizes<O, W><<<grid_persistent(L.n, 8), BLOCK, hist ? (size_t)k * sizeof(W) : 0, s>>>(L.n, L.vw, part, k, sizes, hist); count_launch();
         JET_LAUNCH_CHECK();
     }
 
     W sum_vw(const Level<O, E, W>& L) {
         W* out = e.template dslot<W>(51);
         JET_CUDA(cudaMemsetAsync(out, 0, sizeof(int64_t), s));
-        k_sum<W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(L.vw, L.n, out);
+        k_sum<W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(L.vw, L.n, out); count_launch();
         JET_LAUNCH_CHECK();
         JET_CUDA(cudaMemcpyAsync(&e.hscal[0], out, sizeof(W), cudaMemcpyDeviceToHost, s));
         e.sync();
@@ -278,7 +303,7 @@ struct Refiner {
     void check_parts(const Level<O, E, W>& L, const part_t* part) {
         int* err = e.template dslot<int>(52);
         JET_CUDA(cudaMemsetAsync(err, 0, sizeof(int64_t), s));
-        k_check_parts<<<grid_persistent(L.n, 8), BLOCK, 0, s>>>((int64_t)L.n, part, k, err);
+        k_check_parts<<<grid_persistent(L.n, 8), BLOCK, 0, s>>>((int64_t)L.n, part, k, err); count_launch();
         JET_LAUNCH_CHECK();
         JET_CUDA(cudaMemcpyAsync(&e.hscal[0], err, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         e.sync();
@@ -500,7 +525,7 @@ W run_partition(Engine<O, E, W>& eng, const Cfg& cfg, const GraphIn<O, E, W>& in
         if (st && idx < JET_MAX_LEVELS) st->levels[idx] = cl;
         if (l > 0) {
             Level<O, E, W>& fine = *levels[l - 1];
-            k_project<O><<<grid_persistent(fine.n, 16), BLOCK, 0, s>>>(fine.n, levels[l]->map.p, cur_part, other);
+            k_project<O><<<grid_persistent(fine.n, 16), BLOCK, 0, s>>>(fine.n, levels[l]->map.p, cur_part, other); count_launch();
             JET_LAUNCH_CHECK();
             std::swap(cur_part, other);
             if (l - 1 > 0) { levels[l].reset(); }
