@@ -150,6 +150,21 @@ int jet_pstat(int tier, int64_t n, int64_t nnz, const void* row_map, const void*
 /* Projection to the finer level (src/uncoarsen.hpp:82-86): fine[i] = coarse[map[i]]. */
 int jet_project(int tier, int64_t n_fine, const void* map, const int32_t* coarse, int32_t* fine, void* stream);
 
+/* Same results as jet_pstat, for callers that must not trigger any device
+ * allocation: code recording into a CUDA stream capture (where cudaMalloc is
+ * illegal) and services that reserve device memory up front and forbid the
+ * library from allocating later.  No counterpart in the reference.
+ * Scratch is a fixed array of about 256 KiB that the library reserves on every
+ * GPU that loads it, held until the process exits.  Limits: num_parts k <= 16384
+ * (JET_ERR_INVALID beyond), part ids must lie in [0, k).  The first call on a
+ * device looks up the array's device address; make that first call before
+ * any stream capture.  Every call shares the array, so calls that overlap on
+ * the GPU (different streams, no ordering between them) race and must be
+ * serialised by the caller.  Graph arrays and part[] are device pointers;
+ * out[6] is host memory; stream NULL means the legacy default stream. */
+int jet_pstat_noalloc(int tier, int64_t n, int64_t nnz, const void* row_map, const void* entries, const void* values,
+                      const void* vweights, const int32_t* part, int32_t k, int64_t* out, void* stream);
+
 /* ---------------------------------------------------------------- runtime
  * Library version string, last error message (thread-local), device sanity. */
 const char* jet_version(void);

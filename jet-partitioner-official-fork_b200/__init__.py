@@ -53,7 +53,7 @@ MEASUREMENT_NAMES = [  # header/experiment_data.hpp:77-98
 EXPORTED_SYMBOLS = [
     "jet_partition_i32", "jet_partition_big", "jet_partition_biggest", "jet_coarsen_map", "jet_contract",
     "jet_conn_build", "jet_refine_iters", "jet_refine_level", "jet_pstat", "jet_project", "jet_version",
-    "jet_last_error", "jet_device_ok", "jet_prof_enable", "jet_prof_read", "jet_launch_count",
+    "jet_last_error", "jet_device_ok", "jet_prof_enable", "jet_prof_read", "jet_launch_count", "jet_pstat_noalloc",
 ]
 
 
@@ -407,6 +407,20 @@ def pstat(g: CSRGraph, part: torch.Tensor, k: int):
     out = (ctypes.c_int64 * 6)()
     _check(load().jet_pstat(TIER_ID[g.tier], ctypes.c_int64(g.n), ctypes.c_int64(g.nnz), _ptr(g.row), _ptr(g.adj),
                             _ptr(g.val), _ptr(g.vw), _ptr(part), int(k), out, _stream_ptr()))
+    return list(out)
+
+
+def pstat_noalloc(g: CSRGraph, part: torch.Tensor, k: int):
+    """pstat without any device allocation by the library (jet_pstat_noalloc):
+    for callers that record into a stream capture or forbid allocation after
+    start-up.  Same six numbers as ``pstat``; k <= 16384.  The graph and part
+    must already be on the device."""
+    _require_cuda()
+    if not (g.row.is_cuda and part.is_cuda):
+        raise JetError(JET_ERR_INVALID, "pstat_noalloc takes device tensors")
+    out = (ctypes.c_int64 * 6)()
+    _check(load().jet_pstat_noalloc(TIER_ID[g.tier], ctypes.c_int64(g.n), ctypes.c_int64(g.nnz), _ptr(g.row),
+                                    _ptr(g.adj), _ptr(g.val), _ptr(g.vw), _ptr(part), int(k), out, _stream_ptr()))
     return list(out)
 
 

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libjetb200.so")
 BUILD = os.path.join(HERE, "_build")
-UNITS = ["runtime.cu", "tier_i32.cu", "tier_big.cu", "tier_biggest.cu"]
+UNITS = ["runtime.cu", "tier_i32.cu", "tier_big.cu", "tier_biggest.cu", "noalloc.cu"]
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 METIS = os.path.join(CUDA, "targets", "x86_64-linux", "lib", "libmetis_static.a")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
