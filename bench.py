@@ -183,11 +183,13 @@ def main():
     g = wl["make"](jet.graphs, dev)
     cfg = jet.config_t(coarsening_alg=wl["alg"], num_parts=wl["k"], max_imb_ratio=wl["imb"])
     part_fn = getattr(jet, PART_FN[wl["tier"]])
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library's kernels and the timing events share it
+    stream = torch.cuda.Stream(device=dev)
+    torch.cuda.set_stream(stream)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)
 
     for s in range(args.warmup):
-        part_fn(cfg, g, seed=100 + s)
+        part_fn(cfg, g, seed=100 + s, stream=stream)
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()

@@ -108,8 +108,10 @@ int partition_impl(const jet_config_c* cfg, O n, const E* row, const O* adj, con
         auto t0 = clk::now();
         Inputs<O, E, W> in;
         in.load(n, row, adj, val, vw, mem, s);
+        double t_load = since(t0);
         validate<O, E, W>(eng, n, in.m, in.prow, in.padj, in.pval, in.pvw);
         double t_transfer = since(t0);
+        if (getenv("JET_DEBUG_TIMING")) fprintf(stderr, "jet: load %.3f ms validate %.3f ms\n", t_load * 1e3, (t_transfer - t_load) * 1e3);
         if (n == 0) { *cut_out = 0; return JET_OK; }
         DBuf<part_t> part_dev;
         part_t* pout = part_out;

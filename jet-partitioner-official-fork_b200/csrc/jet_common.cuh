@@ -126,7 +126,22 @@ template <class T> __host__ __device__ __forceinline__ T ceil_div(T a, T b) { re
 
 // ------------------------------------------------------------------ launch geometry
 // Every kernel launch site calls count_launch() (read by jet_launch_count).
+// While a graph is being captured the count is provisional: the capturing
+// code corrects it by the number of times the captured kernels ran.
 void count_launch();
+int64_t launch_counter();
+void add_launches(int64_t n);
+// True while this thread captures work into a CUDA graph (profiling event
+// records are skipped: they are not allowed inside conditional bodies).
+bool& capturing();
+// Per-device stream used only to capture graphs.
+cudaStream_t capture_stream();
+// Pinned, device-mapped host buffers reused across calls (cudaHostAlloc costs
+// milliseconds): acquire returns a slot of at least `bytes`, release frees it
+// for reuse by a later caller on the same thread.
+int pinned_acquire(size_t bytes);
+void* pinned_ptr(int slot);
+void pinned_release(int slot);
 
 struct Dev {
     int sms = 148;

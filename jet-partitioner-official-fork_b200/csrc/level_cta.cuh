@@ -1,0 +1,209 @@
+// level_cta.cuh -- the whole refinement loop of a small level in one CTA.
+//
+// For levels of at most CTA_MAX_N vertices the per-iteration work is a few
+// microseconds of memory traffic, and a loop of separate kernel launches is
+// bound by launch and dependency latency.  Here one 1024-thread block runs
+// jet_refine's loop (src/jet_refiner.hpp:1094-1134) end to end: every phase
+// is the same device function the grid kernels use, separated by
+// __syncthreads instead of kernel boundaries, and the rebalance tail (bucket
+// offsets, candidate order, eviction scores, destination draws) is done in
+// shared memory.  Results are identical to the multi-kernel path.
+#pragma once
+#include "refine.cuh"
+
+namespace jetb {
+
+static constexpr int CTA_MAX_N = 16384;   // candidate sort buffer: CTA_MAX_N x 8 B in shared memory
+static constexpr int CTA_MAX_K = 256;     // per-warp connectivity tables: 32 warps x k slots
+static constexpr int CTA_THREADS = 1024;
+
+template <class O>
+struct LevelLists {
+    const O* warp_list;
+    O n_warp;
+    const O* hub_list;
+    O n_hub;
+    int group;
+};
+
+// Exclusive scan of in[0..n) into out (may alias), over the block.
+template <class T>
+__device__ __forceinline__ void block_scan_global(const T* in, T* out, int64_t n) {
+    __shared__ T sw[32];
+    T carry = 0;
+    for (int64_t base = 0; base < n; base += blockDim.x) {
+        int64_t i = base + threadIdx.x;
+        T v = i < n ? in[i] : T(0);
+        T tot;
+        T ex = block_exclusive_scan<T>(v, sw, tot);
+        if (i < n) out[i] = carry + ex;
+        carry += tot;
+    }
+    __syncthreads();
+}
+
+// Bucket offsets, candidates in (bucket, vertex) order and their eviction
+// scores: the block-level form of sort_candidates + k_evict_sorted (+ the
+// strong rebalance's cookie cutter and destination draws).
+template <bool STRONG, class O, class E, class W>
+__device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb, uint64_t* keys, int P) {
+    __shared__ W sw[32];
+    const O n = a.g.n;
+    block_scan_global<W>(rb.buckets, rb.boff, (int64_t)rb.t_minibuckets + 1);
+    for (int i = threadIdx.x; i < P; i += blockDim.x) {
+        uint64_t key = ~0ull;
+        if (i < n) {
+            O b = rb.bid[i];
+            key = ((uint64_t)(b < 0 ? rb.none_key : (uint32_t)b) << 32) | (uint32_t)i;
+        }
+        keys[i] = key;
+    }
+    if (STRONG) for (int p = threadIdx.x; p < a.k; p += blockDim.x) rb.evict_adjust[p] = 0;
+    __syncthreads();
+    block_sort_keys<uint64_t>(keys, P);
+    W carry = 0;
+    for (int base = 0; base < (int)n; base += blockDim.x) {
+        int q = base + threadIdx.x;
+        uint32_t key = q < (int)n ? (uint32_t)(keys[q] >> 32) : rb.none_key;
+        bool cand = key != rb.none_key;
+        O i = cand ? (O)(uint32_t)(keys[q] & 0xffffffffu) : 0;
+        W w = cand ? a.g.vw[i] : (W)0;
+        W tot;
+        W ex = block_exclusive_scan<W>(w, sw, tot);
+        bool take = false;
+        if (cand) {
+            O b = (O)key;
+            part_t p = a.part[i];
+            O begin = (O)p * rb.width;
+            W within = carry + ex - bucket_start<O, W>(rb, b);
+            if (STRONG) rb.score[i] = within;
+            W score = within + bucket_pos<O, W>(rb, b) - bucket_pos<O, W>(rb, begin);
+            W limit = a.sizes[p] - rb.size_max;
+            if (score < limit) {
+                take = true;
+                if (STRONG && score + w >= limit) rb.evict_adjust[p] = score + w;
+            }
+        }
+        O s = warp_append(&a.dev->nmoves, take);
+        if (take) a.moves[s] = i;
+        carry += tot;
+    }
+    __syncthreads();
+    if (STRONG) {
+        d_cookie<O, E, W>(a, rb);
+        __syncthreads();
+        d_strong_first<O, E, W>(a, rb);
+        __syncthreads();
+        d_strong_redraw<O, E, W>(a, rb);
+        __syncthreads();
+    }
+}
+
+template <class O, class E, class W>
+__device__ __forceinline__ void cta_zero_buckets(const RebArgs<O, W>& rb) {
+    int64_t m = (int64_t)rb.t_minibuckets + 1 + rb.width;
+    for (int64_t i = threadIdx.x; i < m; i += blockDim.x) rb.buckets[i] = 0;
+    __syncthreads();
+}
+
+template <int G, class O, class E, class W>
+__device__ __forceinline__ void cta_afterburn(RefArgs<O, E, W>& a) { d_afterburn<G, O, E, W>(a); }
+
+template <class O, class E, class W>
+__global__ void __launch_bounds__(CTA_THREADS, 1)
+k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, W> rbs, Ctl<W>* c, part_t* best_part,
+            W* sizes_best, int P, int max_iters) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint64_t* keys = (uint64_t*)smem_raw;
+    __shared__ int s_mode, s_more, s_copy;
+    const O n = a.g.n;
+    if (threadIdx.x == 0) {
+        ctl_begin_logic(c);
+        s_mode = c->mode;
+        s_more = c->more;
+    }
+    __syncthreads();
+    int iters = 0;
+    while (s_more) {
+        const int mode = s_mode;
+        if (mode == MODE_LP) {
+            d_lp_select_thread<O, E, W>(a);
+            d_lp_select_warp<O, E, W>(a, li.warp_list, li.n_warp);
+            d_lp_select_warp<O, E, W>(a, li.hub_list, li.n_hub);
+            __syncthreads();
+            switch (li.group) {
+                case 4: d_afterburn<4, O, E, W>(a); break;
+                case 8: d_afterburn<8, O, E, W>(a); break;
+                case 16: d_afterburn<16, O, E, W>(a); break;
+                default: d_afterburn<32, O, E, W>(a); break;
+            }
+            __syncthreads();
+            d_afterburn_hub<O, E, W>(a);
+            __syncthreads();
+        } else if (mode == MODE_WEAK) {
+            cta_zero_buckets<O, E, W>(rbw);
+            d_weak_prep<O, E, W>(a, rbw);
+            __syncthreads();
+            d_weak_select_thread<O, E, W>(a, rbw);
+            d_weak_select_warp<O, E, W>(a, rbw, li.warp_list, li.n_warp);
+            d_weak_select_warp<O, E, W>(a, rbw, li.hub_list, li.n_hub);
+            __syncthreads();
+            d_reb_tail<false, O, E, W>(a, rbw, keys, P);
+        } else {
+            cta_zero_buckets<O, E, W>(rbs);
+            d_strong_prep<O, E, W>(a, rbs);
+            __syncthreads();
+            d_strong_score_thread<O, E, W>(a, rbs);
+            d_strong_score_warp<O, E, W>(a, rbs, li.warp_list, li.n_warp);
+            d_strong_score_warp<O, E, W>(a, rbs, li.hub_list, li.n_hub);
+            __syncthreads();
+            d_reb_tail<true, O, E, W>(a, rbs, keys, P);
+        }
+        // perform_moves (src/jet_refiner.hpp:905-955)
+        d_apply_moves<O, E, W>(a, 0);
+        __syncthreads();
+        switch (li.group) {
+            case 4: d_update_small<4, false, O, E, W>(a); break;
+            case 8: d_update_small<8, false, O, E, W>(a); break;
+            case 16: d_update_small<16, false, O, E, W>(a); break;
+            default: d_update_small<32, false, O, E, W>(a); break;
+        }
+        d_update_small_hub<false, O, E, W>(a);
+        __syncthreads();
+        switch (li.group) {
+            case 4: d_update_small<4, true, O, E, W>(a); d_mark_neighbors<4, O, E, W>(a); break;
+            case 8: d_update_small<8, true, O, E, W>(a); d_mark_neighbors<8, O, E, W>(a); break;
+            case 16: d_update_small<16, true, O, E, W>(a); d_mark_neighbors<16, O, E, W>(a); break;
+            default: d_update_small<32, true, O, E, W>(a); d_mark_neighbors<32, O, E, W>(a); break;
+        }
+        d_update_small_hub<true, O, E, W>(a);
+        __syncthreads();
+        d_conn_warp<O, E, W>(a, nullptr, n, 1, &a.dev->large);  // update_large: rebuild marked rows
+        __syncthreads();
+        d_cut_after<O, E, W>(a);
+        __syncthreads();
+        W mx = block_max_sizes<W>(a.sizes, a.k);
+        if (threadIdx.x == 0) {
+            ctl_end_logic<O, W>(c, a.dev, mx);
+            s_mode = c->mode;
+            s_more = c->more && ++iters < max_iters;
+            s_copy = c->copy;
+            if (c->more && iters >= max_iters) atomicOr(&a.dev->err, ERRF_SPIN);
+        }
+        __syncthreads();
+        if (s_copy) {
+            for (int64_t i = threadIdx.x; i < n; i += blockDim.x) best_part[i] = a.part[i];
+            for (int p = threadIdx.x; p < a.k; p += blockDim.x) sizes_best[p] = a.sizes[p];
+        }
+        __syncthreads();
+    }
+}
+
+template <class O, class W>
+constexpr size_t level_cta_smem(int P, int k) {
+    size_t sort_b = (size_t)P * 8;
+    size_t conn_b = (((size_t)(CTA_THREADS / 32) * k * sizeof(part_t) + 15) & ~(size_t)15) + (size_t)(CTA_THREADS / 32) * k * sizeof(W);
+    return sort_b > conn_b ? sort_b : conn_b;
+}
+
+}  // namespace jetb

@@ -40,17 +40,17 @@ struct Engine {
     DBuf<int64_t> dscal;   // small device scalars
     int64_t* hscal = nullptr;  // pinned mirror
     IterResult* hres = nullptr;
-    int seed_level_base = 0;
+    int slot0 = -1;
 
     explicit Engine(cudaStream_t st) : s(st) {
         dscal.alloc(64, s);
-        JET_CUDA(cudaHostAlloc((void**)&hscal, 64 * sizeof(int64_t), cudaHostAllocMapped));
-        JET_CUDA(cudaHostAlloc((void**)&hres, sizeof(IterResult), cudaHostAllocMapped));
+        slot0 = pinned_acquire(64 * sizeof(int64_t) + sizeof(IterResult) + 64);
+        hscal = (int64_t*)pinned_ptr(slot0);
+        hres = (IterResult*)(hscal + 64);
     }
     ~Engine() {
         cudaStreamSynchronize(s);
-        if (hscal) cudaFreeHost(hscal);
-        if (hres) cudaFreeHost(hres);
+        pinned_release(slot0);
     }
     template <class T> T* dslot(int i) { return (T*)(dscal.p + i); }
     void sync() { JET_CUDA(cudaStreamSynchronize(s)); }

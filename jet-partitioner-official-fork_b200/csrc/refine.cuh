@@ -82,6 +82,7 @@ struct RefArgs {
     O* moves;
     O* moves_hub;
     RefDev<O, W>* dev;
+    const double* filter;  // LP filter ratio, read on the device (it changes per iteration with ultra settings)
 };
 
 // ---------------------------------------------------------------- table build
@@ -208,16 +209,17 @@ __device__ __forceinline__ void smem_table_flush(const part_t* keys, const W* va
 // 32 < deg <= 4096 and k <= WARP_TABLE: one warp per vertex, table in shared memory.
 static constexpr int WARP_TABLE = 512;
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_conn_warp(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) {
+__device__ __forceinline__ void d_conn_warp(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (gate && !*gate) return;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int kw = a.k < WARP_TABLE ? a.k : WARP_TABLE;
+    const int nw = (int)(blockDim.x >> 5);
     part_t* keys = (part_t*)smem_raw + wid * kw;
-    W* vals = (W*)(smem_raw + (BLOCK / 32) * kw * sizeof(part_t) + ((BLOCK / 32) * kw * sizeof(part_t)) % 8) + wid * kw;
-    const int64_t warps = (int64_t)gridDim.x * (BLOCK / 32);
-    for (int64_t x = blockIdx.x * (int64_t)(BLOCK / 32) + wid; x < count; x += warps) {
-        O i = list[x];
+    W* vals = (W*)(smem_raw + (((size_t)nw * kw * sizeof(part_t) + 15) & ~(size_t)15)) + wid * kw;
+    const int64_t warps = (int64_t)gridDim.x * nw;
+    for (int64_t x = blockIdx.x * (int64_t)nw + wid; x < count; x += warps) {
+        O i = list ? list[x] : (O)x;  // no list: every vertex
         if (only_marked && !a.mark[i]) continue;
         E rs = a.g.row[i], re = a.g.row[i + 1];
         part_t cap = conn_cap<E>(re - rs, a.k);
@@ -232,10 +234,12 @@ __global__ void __launch_bounds__(BLOCK) k_conn_warp(RefArgs<O, E, W> a, const O
         __syncwarp();
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_conn_warp(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) { d_conn_warp<O, E, W>(a, list, count, only_marked, gate); }
 
 // Any degree: one CTA per vertex, table of cap <= k slots in shared memory.
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) {
+__device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_used;
     if (gate && !*gate) return;
@@ -259,6 +263,8 @@ __global__ void __launch_bounds__(1024) k_conn_cta(RefArgs<O, E, W> a, const O* 
         __syncthreads();
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) { d_conn_cta<O, E, W>(a, list, count, only_marked, gate); }
 
 // ---------------------------------------------------------------- lookups
 template <class W>
@@ -297,8 +303,9 @@ __device__ __forceinline__ void lp_finish(const RefArgs<O, E, W>& a, O i, part_t
 }
 
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_lp_select_thread(RefArgs<O, E, W> a, double filter_ratio) {
+__device__ __forceinline__ void d_lp_select_thread(RefArgs<O, E, W> a) {
     const W GAIN_MIN = std::numeric_limits<W>::lowest();
+    const double filter_ratio = *a.filter;
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t rounds = ceil_div<int64_t>((int64_t)a.g.n, stride);
@@ -332,14 +339,17 @@ __global__ void __launch_bounds__(BLOCK) k_lp_select_thread(RefArgs<O, E, W> a, 
         if (cand) a.cand[s] = i;
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_lp_select_thread(RefArgs<O, E, W> a) { d_lp_select_thread<O, E, W>(a); }
 
 // Vertices with deg > 32: one warp per vertex scans its table.
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_lp_select_warp(RefArgs<O, E, W> a, const O* list, O count, double filter_ratio) {
+__device__ __forceinline__ void d_lp_select_warp(RefArgs<O, E, W> a, const O* list, O count) {
     const W GAIN_MIN = std::numeric_limits<W>::lowest();
+    const double filter_ratio = *a.filter;
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (BLOCK / 32);
-    for (int64_t x = blockIdx.x * (int64_t)(BLOCK / 32) + (threadIdx.x >> 5); x < count; x += warps) {
+    const int64_t warps = (int64_t)gridDim.x * (int)(blockDim.x >> 5);
+    for (int64_t x = blockIdx.x * (int64_t)(int)(blockDim.x >> 5) + (threadIdx.x >> 5); x < count; x += warps) {
         O i = list[x];
         part_t best = a.dest_cache[i];
         if (best != NULL_PART) {
@@ -379,6 +389,8 @@ __global__ void __launch_bounds__(BLOCK) k_lp_select_warp(RefArgs<O, E, W> a, co
         }
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_lp_select_warp(RefArgs<O, E, W> a, const O* list, O count) { d_lp_select_warp<O, E, W>(a, list, count); }
 
 // ---------------------------------------------------------------- afterburner
 // src/jet_refiner.hpp:275-307: a candidate keeps its move if its gain,
@@ -400,7 +412,7 @@ __device__ __forceinline__ W afterburn_edge(const RefArgs<O, E, W>& a, O i, W ig
 }
 
 template <int G, class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_afterburn(RefArgs<O, E, W> a) {
+__device__ __forceinline__ void d_afterburn(RefArgs<O, E, W> a) {
     O count = a.dev->ncand;
 #define AB_BODY(x, in, lane)                                                                \
     {                                                                                       \
@@ -422,9 +434,11 @@ __global__ void __launch_bounds__(BLOCK) k_afterburn(RefArgs<O, E, W> a) {
     JET_GROUP_LOOP(G, count, AB_BODY)
 #undef AB_BODY
 }
+template <int G, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_afterburn(RefArgs<O, E, W> a) { d_afterburn<G, O, E, W>(a); }
 
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_afterburn_hub(RefArgs<O, E, W> a) {
+__device__ __forceinline__ void d_afterburn_hub(RefArgs<O, E, W> a) {
     __shared__ W part_sum[32];
     O count = a.dev->ncand_hub;
     for (O x = blockIdx.x; x < count; x += gridDim.x) {
@@ -447,6 +461,8 @@ __global__ void __launch_bounds__(1024) k_afterburn_hub(RefArgs<O, E, W> a) {
         __syncthreads();
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_afterburn_hub(RefArgs<O, E, W> a) { d_afterburn_hub<O, E, W>(a); }
 
 // ---------------------------------------------------------------- gain buckets
 // src/jet_refiner.hpp:326-356 with C++ semantics kept: the float gain is
@@ -526,7 +542,7 @@ struct GetSortedWeight {
 
 // Undersized parts in index order (src/jet_refiner.hpp:584-598).
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_weak_prep(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_weak_prep(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     __shared__ int sw[32];
     int carry = 0;
     for (int base = 0; base < a.k; base += 1024) {
@@ -539,6 +555,8 @@ __global__ void __launch_bounds__(1024) k_weak_prep(RefArgs<O, E, W> a, RebArgs<
     }
     if (threadIdx.x == 0) a.dev->total_undersized = carry;
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_weak_prep(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_weak_prep<O, E, W>(a, rb); }
 
 // Destination choice and bucket score (src/jet_refiner.hpp:599-645), one
 // thread per vertex (tables of vertices with deg > 32 are scanned by a warp).
@@ -566,7 +584,7 @@ __device__ __forceinline__ void weak_score(const RefArgs<O, E, W>& a, const RebA
 }
 
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_weak_select_thread(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_weak_select_thread(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < a.g.n; x += (int64_t)gridDim.x * blockDim.x) {
         O i = (O)x;
         if (a.g.row[i + 1] - a.g.row[i] > THREAD_DEG) continue;
@@ -589,12 +607,14 @@ __global__ void __launch_bounds__(BLOCK) k_weak_select_thread(RefArgs<O, E, W> a
         weak_score<O, E, W>(a, rb, i, p, best, gain, p_gain, elig);
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_weak_select_thread(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_weak_select_thread<O, E, W>(a, rb); }
 
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_weak_select_warp(RefArgs<O, E, W> a, RebArgs<O, W> rb, const O* list, O count) {
+__device__ __forceinline__ void d_weak_select_warp(RefArgs<O, E, W> a, RebArgs<O, W> rb, const O* list, O count) {
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (BLOCK / 32);
-    for (int64_t x = blockIdx.x * (int64_t)(BLOCK / 32) + (threadIdx.x >> 5); x < count; x += warps) {
+    const int64_t warps = (int64_t)gridDim.x * (int)(blockDim.x >> 5);
+    for (int64_t x = blockIdx.x * (int64_t)(int)(blockDim.x >> 5) + (threadIdx.x >> 5); x < count; x += warps) {
         O i = list[x];
         part_t p = a.part[i];
         W sp = a.sizes[p];
@@ -622,10 +642,12 @@ __global__ void __launch_bounds__(BLOCK) k_weak_select_warp(RefArgs<O, E, W> a, 
         if (lane == 0) weak_score<O, E, W>(a, rb, i, p, best, gain, p_gain, elig);
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_weak_select_warp(RefArgs<O, E, W> a, RebArgs<O, W> rb, const O* list, O count) { d_weak_select_warp<O, E, W>(a, rb, list, count); }
 
 // max_vwgt: largest room left in a part below max_dest (src/jet_refiner.hpp:442-451).
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_strong_prep(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_strong_prep(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     __shared__ W sm[32];
     __shared__ int sany[32];
     W best = std::numeric_limits<W>::lowest();
@@ -649,6 +671,8 @@ __global__ void __launch_bounds__(1024) k_strong_prep(RefArgs<O, E, W> a, RebArg
         a.dev->total_undersized = any;
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_strong_prep(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_strong_prep<O, E, W>(a, rb); }
 
 // Eviction score: average loss to adjacent non-full parts (unsigned
 // division, src/jet_refiner.hpp:452-480).
@@ -677,7 +701,7 @@ __device__ __forceinline__ bool strong_eligible(const RefArgs<O, E, W>& a, const
 }
 
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_strong_score_thread(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_strong_score_thread(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < a.g.n; x += (int64_t)gridDim.x * blockDim.x) {
         O i = (O)x;
         if (a.g.row[i + 1] - a.g.row[i] > THREAD_DEG) continue;
@@ -696,12 +720,14 @@ __global__ void __launch_bounds__(BLOCK) k_strong_score_thread(RefArgs<O, E, W> 
         strong_score<O, E, W>(a, rb, i, p, tg, tk, p_gain);
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_strong_score_thread(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_strong_score_thread<O, E, W>(a, rb); }
 
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_strong_score_warp(RefArgs<O, E, W> a, RebArgs<O, W> rb, const O* list, O count) {
+__device__ __forceinline__ void d_strong_score_warp(RefArgs<O, E, W> a, RebArgs<O, W> rb, const O* list, O count) {
     const int lane = threadIdx.x & 31;
-    const int64_t warps = (int64_t)gridDim.x * (BLOCK / 32);
-    for (int64_t x = blockIdx.x * (int64_t)(BLOCK / 32) + (threadIdx.x >> 5); x < count; x += warps) {
+    const int64_t warps = (int64_t)gridDim.x * (int)(blockDim.x >> 5);
+    for (int64_t x = blockIdx.x * (int64_t)(int)(blockDim.x >> 5) + (threadIdx.x >> 5); x < count; x += warps) {
         O i = list[x];
         part_t p = a.part[i];
         if (lane == 0) rb.bid[i] = -1;
@@ -721,13 +747,19 @@ __global__ void __launch_bounds__(BLOCK) k_strong_score_warp(RefArgs<O, E, W> a,
         if (lane == 0) strong_score<O, E, W>(a, rb, i, p, tg, tk, p_gain);
     }
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_strong_score_warp(RefArgs<O, E, W> a, RebArgs<O, W> rb, const O* list, O count) { d_strong_score_warp<O, E, W>(a, rb, list, count); }
 
 // get_evictions (src/jet_refiner.hpp:392-409).  The reference's in-bucket
 // score is an atomic fetch-add whose order, run in index order, is the
 // weight of the bucket's earlier vertices; here it is read off the stable
 // sort by bucket id: wpre[q] - (weight of all earlier buckets).
 template <bool ADJUST, class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_evict_sorted(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_evict_sorted(RefArgs<O, E, W> a, RebArgs<O, W> rb);
+template <bool ADJUST, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_evict_sorted(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_evict_sorted<ADJUST, O, E, W>(a, rb); }
+template <bool ADJUST, class O, class E, class W>
+__device__ __forceinline__ void d_evict_sorted(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t rounds = ceil_div<int64_t>((int64_t)a.g.n, stride);
@@ -757,7 +789,7 @@ __global__ void __launch_bounds__(BLOCK) k_evict_sorted(RefArgs<O, E, W> a, RebA
 // "cookie cutter" (src/jet_refiner.hpp:491-518): prefix positions of the
 // evicted weight per part and of the free room per undersized part.
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_cookie(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_cookie(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     __shared__ W sw[32];
     W carry = 0;
     for (int base = 0; base < a.k; base += 1024) {
@@ -786,13 +818,15 @@ __global__ void __launch_bounds__(1024) k_cookie(RefArgs<O, E, W> a, RebArgs<O, 
     }
     if (threadIdx.x == 0) rb.evict_start[0] = 0;
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_cookie(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_cookie<O, E, W>(a, rb); }
 
 // Adjust scores and pick destinations by chunk (src/jet_refiner.hpp:519-544).
 // A vertex less than half inside its chunk draws a new position past the
 // end; only those draws depend on order (they advance one shared cursor),
 // so they are queued here and replayed in vertex order by k_strong_redraw.
 template <class O, class E, class W>
-__global__ void k_strong_first(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_strong_first(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     O count = a.dev->nmoves;
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < count; x += (int64_t)gridDim.x * blockDim.x) {
         O v = a.moves[x];
@@ -816,6 +850,8 @@ __global__ void k_strong_first(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
         a.dest[v] = dest;
     }
 }
+template <class O, class E, class W>
+__global__ void k_strong_first(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_strong_first<O, E, W>(a, rb); }
 
 // One block: sorts the queued vertices by id and replays their draws in order.
 static constexpr int REDRAW_CAP = 4096;
@@ -836,7 +872,7 @@ __device__ __forceinline__ void block_sort_keys(K* key, int P) {
     }
 }
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     __shared__ O list[REDRAW_CAP];
     O cnt = a.dev->nredraw;
     if (cnt == 0) return;
@@ -870,12 +906,14 @@ __global__ void __launch_bounds__(1024) k_strong_redraw(RefArgs<O, E, W> a, RebA
     }
     a.dev->vw_cursor = cursor;
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_strong_redraw<O, E, W>(a, rb); }
 
 // ---------------------------------------------------------------- moves
 // perform_moves part 1 (src/jet_refiner.hpp:910-931): cut change from the old
 // tables, apply the moves, part-size deltas through a shared histogram.
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_apply_moves(RefArgs<O, E, W> a, int hist) {
+__device__ __forceinline__ void d_apply_moves(RefArgs<O, E, W> a, int hist) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     W* hs = (W*)smem_raw;
     if (hist) {
@@ -907,6 +945,8 @@ __global__ void __launch_bounds__(BLOCK) k_apply_moves(RefArgs<O, E, W> a, int h
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) a.dev->large = count > (O)(a.g.n / 10);
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_apply_moves(RefArgs<O, E, W> a, int hist) { d_apply_moves<O, E, W>(a, hist); }
 
 // update_small subtract (src/jet_refiner.hpp:786-808).
 template <class O, class E, class W>
@@ -976,7 +1016,7 @@ __device__ __forceinline__ void conn_add(const RefArgs<O, E, W>& a, O v, part_t 
 }
 
 template <int G, bool ADD, class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_update_small(RefArgs<O, E, W> a) {
+__device__ __forceinline__ void d_update_small(RefArgs<O, E, W> a) {
     if (a.dev->large) return;
     O count = a.dev->nmoves;
 #define UPD_BODY(x, in, lane)                                                               \
@@ -996,9 +1036,11 @@ __global__ void __launch_bounds__(BLOCK) k_update_small(RefArgs<O, E, W> a) {
     JET_GROUP_LOOP(G, count, UPD_BODY)
 #undef UPD_BODY
 }
+template <int G, bool ADD, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_update_small(RefArgs<O, E, W> a) { d_update_small<G, ADD, O, E, W>(a); }
 
 template <bool ADD, class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_update_small_hub(RefArgs<O, E, W> a) {
+__device__ __forceinline__ void d_update_small_hub(RefArgs<O, E, W> a) {
     if (a.dev->large) return;
     O count = a.dev->nmoves_hub;
     for (O x = blockIdx.x; x < count; x += gridDim.x) {
@@ -1010,11 +1052,13 @@ __global__ void __launch_bounds__(1024) k_update_small_hub(RefArgs<O, E, W> a) {
         }
     }
 }
+template <bool ADD, class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_update_small_hub(RefArgs<O, E, W> a) { d_update_small_hub<ADD, O, E, W>(a); }
 
 // update_large (src/jet_refiner.hpp:743-777): mark every neighbour of a
 // moved vertex; the marked rows are rebuilt by the table builders.
 template <int G, class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_mark_neighbors(RefArgs<O, E, W> a) {
+__device__ __forceinline__ void d_mark_neighbors(RefArgs<O, E, W> a) {
     if (!a.dev->large) return;
     O count = a.dev->nmoves;
 #define MARK_BODY(x, in, lane)                                                              \
@@ -1030,11 +1074,13 @@ __global__ void __launch_bounds__(BLOCK) k_mark_neighbors(RefArgs<O, E, W> a) {
     JET_GROUP_LOOP(G, count, MARK_BODY)
 #undef MARK_BODY
 }
+template <int G, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_mark_neighbors(RefArgs<O, E, W> a) { d_mark_neighbors<G, O, E, W>(a); }
 
 // perform_moves part 2 (src/jet_refiner.hpp:937-946): cut change from the
 // updated tables.
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_cut_after(RefArgs<O, E, W> a) {
+__device__ __forceinline__ void d_cut_after(RefArgs<O, E, W> a) {
     O count = a.dev->nmoves;
     W c2 = 0;
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < count; x += (int64_t)gridDim.x * blockDim.x) {
@@ -1046,6 +1092,8 @@ __global__ void __launch_bounds__(BLOCK) k_cut_after(RefArgs<O, E, W> a) {
     c2 = group_sum<W>(c2, 32);
     if ((threadIdx.x & 31) == 0 && c2) atomic_add(&a.dev->cut2, c2);
 }
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_cut_after(RefArgs<O, E, W> a) { d_cut_after<O, E, W>(a); }
 
 // Largest part, results to the host mirror, counters reset.
 template <class O, class E, class W>
@@ -1067,6 +1115,133 @@ __global__ void __launch_bounds__(1024) k_finalize(RefArgs<O, E, W> a, IterResul
         d->ncand = 0; d->nmoves = 0; d->ncand_hub = 0; d->nmoves_hub = 0; d->nredraw = 0;
         d->cut1 = 0; d->cut2 = 0; d->large = 0;
     }
+}
+
+// ---------------------------------------------------------------- device-side control
+// The iteration control of jet_refine (src/jet_refiner.hpp:1094-1134) run on
+// the device, so a whole level refines inside one CUDA graph: a WHILE node
+// repeats the iteration, IF nodes select LP / weak / strong and the copy of
+// an improved state.  State lives in Ctl; handles are set with
+// cudaGraphSetConditional.
+enum { MODE_LP = 0, MODE_WEAK = 1, MODE_STRONG = 2 };
+static constexpr int MAX_TEMPS = 24;
+
+template <class W>
+struct Ctl {
+    W curr_cut, curr_imb, best_cut, best_imb;
+    W opt, imb_max;
+    double tol;
+    double filter;
+    double temps[MAX_TEMPS];
+    int n_temps, temp_idx;
+    int count, balance_counter, lab_counter, iter_count;
+    int weak_iters, strong_iters;
+    int mode, copy, more;
+};
+
+struct CtlHandles {
+    cudaGraphConditionalHandle loop, lp, weak, strong, copy;
+};
+
+// Mode of the next iteration, decided the way the loop body starts
+// (src/jet_refiner.hpp:1106-1117).
+template <class W>
+__device__ __forceinline__ void ctl_next_mode(Ctl<W>* c) {
+    c->iter_count++;
+    if (c->curr_imb <= c->imb_max) {
+        c->mode = MODE_LP;
+        c->balance_counter = 0;
+        c->lab_counter++;
+    } else {
+        c->mode = c->balance_counter < 2 ? MODE_WEAK : MODE_STRONG;
+        if (c->mode == MODE_WEAK) c->weak_iters++; else c->strong_iters++;
+        c->balance_counter++;
+    }
+}
+
+template <class W>
+__device__ __forceinline__ void ctl_set_handles(const Ctl<W>* c, const CtlHandles& h, bool in_graph) {
+    if (!in_graph) return;
+    cudaGraphSetConditional(h.lp, c->more && c->mode == MODE_LP);
+    cudaGraphSetConditional(h.weak, c->more && c->mode == MODE_WEAK);
+    cudaGraphSetConditional(h.strong, c->more && c->mode == MODE_STRONG);
+    cudaGraphSetConditional(h.copy, c->copy);
+    cudaGraphSetConditional(h.loop, c->more);
+}
+
+// Before the first iteration: the first `count++ <= 11` check passes.
+template <class W>
+__device__ __forceinline__ void ctl_begin_logic(Ctl<W>* c) {
+    c->count = 1;
+    c->temp_idx = 0;
+    c->filter = c->temps[0];
+    c->more = 1;
+    c->copy = 0;
+    ctl_next_mode(c);
+}
+template <class W>
+__global__ void k_ctl_begin(Ctl<W>* c, CtlHandles h) {
+    ctl_begin_logic(c);
+    ctl_set_handles(c, h, true);
+}
+
+// After an iteration: applies the cut change and largest part, keeps the best
+// state (src/jet_refiner.hpp:1120-1132), evaluates the loop condition and the
+// next mode, and resets the per-iteration counters.
+template <class O, class W>
+__device__ __forceinline__ void ctl_end_logic(Ctl<W>* c, RefDev<O, W>* d, W mx) {
+    c->curr_cut -= d->cut1 + d->cut2;
+    c->curr_imb = mx > c->opt ? mx - c->opt : 0;
+    c->copy = 0;
+    if (c->best_imb > c->imb_max && c->curr_imb < c->best_imb) {
+        c->best_cut = c->curr_cut;
+        c->best_imb = c->curr_imb;
+        c->copy = 1;
+        c->count = 0;
+    } else if (c->curr_cut < c->best_cut && (c->curr_imb <= c->imb_max || c->curr_imb <= c->best_imb)) {
+        if ((double)c->curr_cut < c->tol * (double)c->best_cut) c->count = 0;
+        c->best_cut = c->curr_cut;
+        c->best_imb = c->curr_imb;
+        c->copy = 1;
+    }
+    int more = 1;
+    if (!(c->count++ <= 11)) {
+        c->temp_idx++;
+        if (c->temp_idx < c->n_temps) {
+            c->filter = c->temps[c->temp_idx];
+            c->count = 1;
+        } else {
+            more = 0;
+        }
+    }
+    c->more = more;
+    if (more) ctl_next_mode(c);
+    d->ncand = 0; d->nmoves = 0; d->ncand_hub = 0; d->nmoves_hub = 0; d->nredraw = 0;
+    d->cut1 = 0; d->cut2 = 0; d->large = 0;
+}
+
+// Largest part size, reduced over the block (result valid in thread 0).
+template <class W>
+__device__ __forceinline__ W block_max_sizes(const W* sizes, int k) {
+    __shared__ W sm[32];
+    W mx = std::numeric_limits<W>::lowest();
+    for (int p = threadIdx.x; p < k; p += blockDim.x) { W s = sizes[p]; if (s > mx) mx = s; }
+    for (int m = 16; m > 0; m >>= 1) { W y = shfl_xor(mx, m, 32); if (y > mx) mx = y; }
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) if (sm[w] > mx) mx = sm[w];
+    __syncthreads();
+    return mx;
+}
+
+// Closes an iteration inside the level graph and sets the graph's handles.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_finalize_ctl(RefArgs<O, E, W> a, Ctl<W>* c, CtlHandles h) {
+    W mx = block_max_sizes<W>(a.sizes, a.k);
+    if (threadIdx.x != 0) return;
+    ctl_end_logic<O, W>(c, a.dev, mx);
+    ctl_set_handles(c, h, true);
 }
 
 // ---------------------------------------------------------------- statistics

@@ -57,6 +57,47 @@ cudaStream_t default_stream() {
 
 static std::atomic<int64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+int64_t launch_counter() { return g_launches.load(); }
+void add_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+bool& capturing() {
+    static thread_local bool c = false;
+    return c;
+}
+
+cudaStream_t capture_stream() {
+    static cudaStream_t streams[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!streams[dev]) JET_CUDA(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
+    return streams[dev];
+}
+
+struct PinnedSlot {
+    void* p = nullptr;
+    size_t bytes = 0;
+    bool used = false;
+};
+static thread_local std::vector<PinnedSlot> g_pinned;
+
+int pinned_acquire(size_t bytes) {
+    for (size_t i = 0; i < g_pinned.size(); i++) {
+        PinnedSlot& sl = g_pinned[i];
+        if (!sl.used && sl.bytes >= bytes) { sl.used = true; return (int)i; }
+    }
+    PinnedSlot sl;
+    size_t b = bytes < 4096 ? 4096 : bytes;
+    JET_CUDA(cudaHostAlloc(&sl.p, b, cudaHostAllocMapped));
+    sl.bytes = b;
+    sl.used = true;
+    g_pinned.push_back(sl);
+    return (int)g_pinned.size() - 1;
+}
+void* pinned_ptr(int slot) { return g_pinned[slot].p; }
+void pinned_release(int slot) {
+    if (slot >= 0 && slot < (int)g_pinned.size()) g_pinned[slot].used = false;
+}
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
@@ -75,7 +116,7 @@ struct ProfState {
 static ProfState g_prof;
 
 int prof_begin(cudaStream_t s) {
-    if (!g_prof.on) return -1;
+    if (!g_prof.on || capturing()) return -1;
     if (g_prof.next + 2 > (int)g_prof.pool.size()) {
         int old = (int)g_prof.pool.size();
         g_prof.pool.resize(old + 512);
@@ -88,7 +129,7 @@ int prof_begin(cudaStream_t s) {
 }
 
 void prof_end(int h, ProfKernel k, double bytes, cudaStream_t s) {
-    if (h < 0 || !g_prof.on) return;
+    if (h < 0 || !g_prof.on || capturing()) return;
     cudaEventRecord(g_prof.pool[h + 1], s);
     g_prof.pending.push_back({h, (int)k, bytes});
 }

@@ -4,6 +4,7 @@
 #pragma once
 #include "partitioner.cuh"
 #include "sort.cuh"
+#include "level_cta.cuh"
 
 namespace jetb {
 
@@ -25,8 +26,13 @@ struct Refiner {
     DBuf<part_t> redraw_p;
     RadixScratch rsort;
     DBuf<RefDev<O, W>> dev;
+    DBuf<Ctl<W>> ctl;
+    Ctl<W>* hctl = nullptr;  // pinned mirror
+    int pslot = -1;
     int64_t bucket_cap = 0;
     bool verbose = false;
+    bool use_graph = true;
+    bool use_cta = true;
 
     struct HostState {
         W cut = 0;
@@ -57,6 +63,22 @@ struct Refiner {
         redraw.alloc(n1, s); redraw_p.alloc(n1, s);
         dev.alloc(1, s);
         dev.zero();
+        ctl.alloc(1, s);
+        ctl.zero();
+        pslot = pinned_acquire(sizeof(Ctl<W>));
+        hctl = (Ctl<W>*)pinned_ptr(pslot);
+        std::memset(hctl, 0, sizeof(Ctl<W>));
+        // scratch for every scan and sort an iteration may run, sized up front
+        // so that iterations can be captured into a graph (no allocation inside)
+        int64_t scan_max = (n1 + 1 > bucket_cap ? n1 + 1 : bucket_cap);
+        int64_t tiles = ceil_div<int64_t>(scan_max, SCAN_TILE) + 1024;
+        if (e.scan.buf.n < tiles) e.scan.buf.alloc(tiles, s);
+        int64_t rs_h = ceil_div<int64_t>(n1, RS_TILE) * RS_BINS + 1024;
+        if (rsort.hist.n < rs_h) rsort.hist.alloc(rs_h, s);
+    }
+    ~Refiner() {
+        cudaStreamSynchronize(s);
+        pinned_release(pslot);
     }
 
     // src/jet_refiner.hpp:425-430 and :559-564
@@ -75,7 +97,7 @@ struct Refiner {
         a.g = L.view(); a.k = k; a.coff = coff.p; a.slots = slots.p; a.csize = csize.p; a.dest_cache = dest_cache.p;
         a.lock = lock.p; a.mark = mark.p; a.part = part_work.p; a.dest = dest.p; a.save_gain = save_gain.p;
         a.pregain = pregain.p; a.sizes = sizes_curr.p; a.cand = cand.p; a.cand_hub = cand_hub.p; a.moves = moves.p;
-        a.moves_hub = moves_hub.p; a.dev = dev.p;
+        a.moves_hub = moves_hub.p; a.dev = dev.p; a.filter = &ctl.p->filter;
         return a;
     }
 
@@ -133,13 +155,13 @@ struct Refiner {
         return (int64_t)C;
     }
 
-    void lp(const Level<O, E, W>& L, double filter_ratio) {
+    void lp(const Level<O, E, W>& L) {
         auto a = args(L);
         int h = prof_begin(s);
-        k_lp_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, filter_ratio); count_launch();
+        k_lp_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a); count_launch();
         JET_LAUNCH_CHECK();
-        if (L.n_warp > 0) k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, L.warp_list.p, L.n_warp, filter_ratio); count_launch();
-        if (L.n_hub > 0) k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, L.hub_list.p, L.n_hub, filter_ratio); count_launch();
+        if (L.n_warp > 0) { k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, L.warp_list.p, L.n_warp); count_launch(); }
+        if (L.n_hub > 0) { k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, L.hub_list.p, L.n_hub); count_launch(); }
         JET_LAUNCH_CHECK();
         prof_end(h, PK_LP_SELECT, 0, s);
         h = prof_begin(s);
@@ -158,7 +180,18 @@ struct Refiner {
         prof_end(h, PK_AFTERBURN, 0, s);
     }
 
-    RebArgs<O, W> reb_args(const Level<O, E, W>& L, W max_dest, W opt, W size_max) {
+    // max_dest of src/jet_refiner.hpp:575-578 (weak) and :437 (strong)
+    static W weak_max_dest(W size_max) {
+        W md = (W)((double)size_max * 0.99);
+        if (md < size_max - 100) md = size_max - 100;
+        return md;
+    }
+    static W strong_max_dest(W opt, W size_max) {
+        W md = (W)((double)size_max * 0.99);
+        return opt + 1 > md ? opt + 1 : md;
+    }
+
+    RebArgs<O, W> reb_args(const Level<O, E, W>& L, W max_dest, W opt, W size_max, bool clear = true) {
         RebArgs<O, W> rb;
         O sections, tmb;
         sections_for(L.n, sections, tmb);
@@ -169,7 +202,7 @@ struct Refiner {
         rb.skey = nullptr; rb.sval = nullptr; rb.wpre = wpre.p;
         rb.none_key = (uint32_t)((int64_t)tmb + rb.width + 1);
         if ((int64_t)tmb + 1 + rb.width > bucket_cap) throw JetError{JET_ERR_INVALID, "bucket array too small"};
-        JET_CUDA(cudaMemsetAsync(buckets.p, 0, sizeof(W) * ((size_t)tmb + 1 + rb.width), s));
+        if (clear) JET_CUDA(cudaMemsetAsync(buckets.p, 0, sizeof(W) * ((size_t)tmb + 1 + rb.width), s));
         return rb;
     }
 
@@ -189,9 +222,7 @@ struct Refiner {
     // rebalance_weak, src/jet_refiner.hpp:551-645.
     void weak(const Level<O, E, W>& L, W opt, W size_max) {
         auto a = args(L);
-        W max_dest = (W)((double)size_max * 0.99);
-        if (max_dest < size_max - 100) max_dest = size_max - 100;
-        auto rb = reb_args(L, max_dest, opt, size_max);
+        auto rb = reb_args(L, weak_max_dest(size_max), opt, size_max);
         k_weak_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
         k_weak_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
         if (L.n_warp > 0) { k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp); count_launch(); }
@@ -205,9 +236,7 @@ struct Refiner {
     // rebalance_strong, src/jet_refiner.hpp:417-546.
     void strong(const Level<O, E, W>& L, W opt, W size_max) {
         auto a = args(L);
-        W md = (W)((double)size_max * 0.99);
-        W max_dest = opt + 1 > md ? opt + 1 : md;
-        auto rb = reb_args(L, max_dest, opt, size_max);
+        auto rb = reb_args(L, strong_max_dest(opt, size_max), opt, size_max);
         k_strong_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
         k_strong_score_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
         if (L.n_warp > 0) { k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp); count_launch(); }
@@ -222,8 +251,9 @@ struct Refiner {
         JET_LAUNCH_CHECK();
     }
 
-    // perform_moves, src/jet_refiner.hpp:905-955.  One host sync.
-    IterResult perform_moves(const Level<O, E, W>& L) {
+    // perform_moves, src/jet_refiner.hpp:905-955: every kernel up to the
+    // cut change from the updated tables.
+    void moves_kernels(const Level<O, E, W>& L) {
         auto a = args(L);
         int hist = (size_t)k * sizeof(W) <= 32 * 1024;
         k_apply_moves<O, E, W><<<grid_persistent(L.n, 8), BLOCK, hist ? (size_t)k * sizeof(W) : 0, s>>>(a, hist); count_launch();
@@ -250,7 +280,13 @@ struct Refiner {
         build_tables(L, 1, &dev.p->large);
         prof_end(h, PK_UPDATE, 0, s);
         k_cut_after<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(a); count_launch();
-        k_finalize<O, E, W><<<1, 1024, 0, s>>>(a, e.hres); count_launch();
+        JET_LAUNCH_CHECK();
+    }
+
+    // Host-driven iteration end: results to pinned memory, one host sync.
+    IterResult perform_moves(const Level<O, E, W>& L) {
+        moves_kernels(L);
+        k_finalize<O, E, W><<<1, 1024, 0, s>>>(args(L), e.hres); count_launch();
         JET_LAUNCH_CHECK();
         e.sync();
         IterResult r = *e.hres;
@@ -346,7 +382,9 @@ struct Refiner {
     int iterate(const Level<O, E, W>& L, const Prob& pb, double filter_ratio, int& balance_counter, int& lab_counter) {
         int kind;
         if (curr.total_imb <= pb.imb_max) {
-            lp(L, filter_ratio);
+            hctl->filter = filter_ratio;
+            JET_CUDA(cudaMemcpyAsync(&ctl.p->filter, &hctl->filter, sizeof(double), cudaMemcpyHostToDevice, s));
+            lp(L);
             balance_counter = 0;
             lab_counter++;
             kind = 0;
@@ -371,6 +409,161 @@ struct Refiner {
         JET_CUDA(cudaMemcpyAsync(best_part, part_work.p, sizeof(part_t) * L.n, cudaMemcpyDeviceToDevice, s));
     }
 
+    // ------------------------------------------------------------ single-CTA loop
+    bool cta_eligible(const Level<O, E, W>& L) const { return use_cta && L.n <= CTA_MAX_N && k <= CTA_MAX_K; }
+
+    void ctl_init(const Prob& pb, const std::vector<double>& temps, double tol) {
+        Ctl<W>& c = *hctl;
+        std::memset(&c, 0, sizeof(c));
+        c.curr_cut = curr.cut; c.curr_imb = curr.total_imb; c.best_cut = best.cut; c.best_imb = best.total_imb;
+        c.opt = pb.opt; c.imb_max = pb.imb_max; c.tol = tol;
+        c.n_temps = (int)(temps.size() < (size_t)MAX_TEMPS ? temps.size() : MAX_TEMPS);
+        for (int i = 0; i < c.n_temps; i++) c.temps[i] = temps[i];
+        JET_CUDA(cudaMemcpyAsync(ctl.p, hctl, sizeof(Ctl<W>), cudaMemcpyHostToDevice, s));
+    }
+
+    void ctl_finish() {
+        JET_CUDA(cudaMemcpyAsync(hctl, ctl.p, sizeof(Ctl<W>), cudaMemcpyDeviceToHost, s));
+        JET_CUDA(cudaMemcpyAsync(e.hres, &dev.p->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+        e.sync();
+        if (*(int*)e.hres & ~16) throw JetError{JET_ERR_OVERFLOW, "refinement exceeded a device bound"};
+        Ctl<W>& c = *hctl;
+        best.cut = c.best_cut;
+        best.total_imb = c.best_imb;
+        curr.cut = c.curr_cut;
+        curr.total_imb = c.curr_imb;
+        total_iters += c.iter_count;
+    }
+
+    void run_level_cta(const Level<O, E, W>& L, part_t* best_part, const Prob& pb, const std::vector<double>& temps, double tol) {
+        ctl_init(pb, temps, tol);
+        LevelLists<O> li{L.warp_list.p, L.n_warp, L.hub_list.p, L.n_hub, L.group};
+        RebArgs<O, W> rbw = reb_args(L, weak_max_dest(pb.size_max), pb.opt, pb.size_max, false);
+        RebArgs<O, W> rbs = reb_args(L, strong_max_dest(pb.opt, pb.size_max), pb.opt, pb.size_max, false);
+        int P = 1;
+        while (P < (int)L.n) P <<= 1;
+        size_t smem = level_cta_smem<O, W>(P, k) + 64;
+        JET_CUDA(cudaFuncSetAttribute(k_level_cta<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_level_cta<O, E, W><<<1, CTA_THREADS, smem, s>>>(args(L), li, rbw, rbs, ctl.p, best_part, sizes_best.p, P, 1 << 22);
+        count_launch();
+        JET_LAUNCH_CHECK();
+        ctl_finish();
+    }
+
+    // ------------------------------------------------------------ graph-resident loop
+    // Captures `fn` (which launches on this->s) into `g` after `deps` on the
+    // capture stream; returns the tail nodes and the number of kernels captured.
+    template <class F>
+    std::vector<cudaGraphNode_t> capture_into(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, F&& fn, int64_t* nkernels) {
+        cudaStream_t cs = capture_stream();
+        JET_CUDA(cudaStreamBeginCaptureToGraph(cs, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                               cudaStreamCaptureModeRelaxed));
+        cudaStream_t saved = s;
+        s = cs;
+        capturing() = true;
+        int64_t l0 = launch_counter();
+        try {
+            fn();
+        } catch (...) {
+            capturing() = false;
+            s = saved;
+            cudaGraph_t dummy;
+            cudaStreamEndCapture(cs, &dummy);
+            throw;
+        }
+        *nkernels = launch_counter() - l0;
+        capturing() = false;
+        s = saved;
+        cudaStreamCaptureStatus st;
+        const cudaGraphNode_t* tail = nullptr;
+        size_t ntail = 0;
+        JET_CUDA(cudaStreamGetCaptureInfo(cs, &st, nullptr, nullptr, &tail, &ntail));
+        std::vector<cudaGraphNode_t> out(tail, tail + ntail);
+        cudaGraph_t gout;
+        JET_CUDA(cudaStreamEndCapture(cs, &gout));
+        return out;
+    }
+
+    static cudaGraphNode_t add_conditional(cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps, cudaGraphConditionalHandle h,
+                                           cudaGraphConditionalNodeType type, cudaGraph_t* body) {
+        cudaGraphNodeParams p = {};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = type;
+        p.conditional.size = 1;
+        cudaGraphNode_t node;
+        JET_CUDA(cudaGraphAddNode(&node, g, deps.empty() ? nullptr : deps.data(), deps.size(), &p));
+        *body = p.conditional.phGraph_out[0];
+        return node;
+    }
+
+    // The refinement loop of one level as one graph launch: no host
+    // round trip per iteration (the reference syncs about three times per
+    // iteration, src/jet_refiner.hpp:199, :416, :550, :904).
+    void run_level_graph(const Level<O, E, W>& L, part_t* best_part, const Prob& pb, const std::vector<double>& temps, double tol) {
+        Ctl<W>& c = *hctl;
+        std::memset(&c, 0, sizeof(c));
+        c.curr_cut = curr.cut; c.curr_imb = curr.total_imb; c.best_cut = best.cut; c.best_imb = best.total_imb;
+        c.opt = pb.opt; c.imb_max = pb.imb_max; c.tol = tol;
+        c.n_temps = (int)(temps.size() < (size_t)MAX_TEMPS ? temps.size() : MAX_TEMPS);
+        for (int i = 0; i < c.n_temps; i++) c.temps[i] = temps[i];
+        JET_CUDA(cudaMemcpyAsync(ctl.p, hctl, sizeof(Ctl<W>), cudaMemcpyHostToDevice, s));
+        set_attrs();
+        cudaGraph_t G;
+        JET_CUDA(cudaGraphCreate(&G, 0));
+        cudaGraphExec_t X = nullptr;
+        try {
+            CtlHandles h;
+            JET_CUDA(cudaGraphConditionalHandleCreate(&h.loop, G, 0, cudaGraphCondAssignDefault));
+            JET_CUDA(cudaGraphConditionalHandleCreate(&h.lp, G, 0, cudaGraphCondAssignDefault));
+            JET_CUDA(cudaGraphConditionalHandleCreate(&h.weak, G, 0, cudaGraphCondAssignDefault));
+            JET_CUDA(cudaGraphConditionalHandleCreate(&h.strong, G, 0, cudaGraphCondAssignDefault));
+            JET_CUDA(cudaGraphConditionalHandleCreate(&h.copy, G, 0, cudaGraphCondAssignDefault));
+            int64_t kb = 0, klp = 0, kw = 0, ks = 0, km = 0;
+            Ctl<W>* cp = ctl.p;
+            auto t0 = capture_into(G, {}, [&] { k_ctl_begin<W><<<1, 1, 0, s>>>(cp, h); count_launch(); JET_LAUNCH_CHECK(); }, &kb);
+            cudaGraph_t body, b_lp, b_weak, b_strong, b_copy;
+            add_conditional(G, t0, h.loop, cudaGraphCondTypeWhile, &body);
+            cudaGraphNode_t n_lp = add_conditional(body, {}, h.lp, cudaGraphCondTypeIf, &b_lp);
+            capture_into(b_lp, {}, [&] { lp(L); }, &klp);
+            cudaGraphNode_t n_weak = add_conditional(body, {n_lp}, h.weak, cudaGraphCondTypeIf, &b_weak);
+            capture_into(b_weak, {}, [&] { weak(L, pb.opt, pb.size_max); }, &kw);
+            cudaGraphNode_t n_strong = add_conditional(body, {n_weak}, h.strong, cudaGraphCondTypeIf, &b_strong);
+            capture_into(b_strong, {}, [&] { strong(L, pb.opt, pb.size_max); }, &ks);
+            auto tm = capture_into(body, {n_strong}, [&] {
+                moves_kernels(L);
+                k_finalize_ctl<O, E, W><<<1, 1024, 0, s>>>(args(L), cp, h); count_launch();
+                JET_LAUNCH_CHECK();
+            }, &km);
+            add_conditional(body, tm, h.copy, cudaGraphCondTypeIf, &b_copy);
+            int64_t kc = 0;
+            capture_into(b_copy, {}, [&] {
+                JET_CUDA(cudaMemcpyAsync(best_part, part_work.p, sizeof(part_t) * L.n, cudaMemcpyDeviceToDevice, s));
+                JET_CUDA(cudaMemcpyAsync(sizes_best.p, sizes_curr.p, sizeof(W) * k, cudaMemcpyDeviceToDevice, s));
+            }, &kc);
+            JET_CUDA(cudaGraphInstantiate(&X, G, 0));
+            JET_CUDA(cudaGraphLaunch(X, s));
+            JET_CUDA(cudaMemcpyAsync(hctl, ctl.p, sizeof(Ctl<W>), cudaMemcpyDeviceToHost, s));
+            JET_CUDA(cudaMemcpyAsync(e.hres, &dev.p->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+            e.sync();
+            // kernels the graph ran: captured once, executed once per iteration of their kind
+            add_launches(kb + klp * c.lab_counter + kw * c.weak_iters + ks * c.strong_iters + km * c.iter_count -
+                         (kb + klp + kw + ks + km));
+        } catch (...) {
+            if (X) cudaGraphExecDestroy(X);
+            cudaGraphDestroy(G);
+            throw;
+        }
+        cudaGraphExecDestroy(X);
+        cudaGraphDestroy(G);
+        if (*(int*)e.hres & ~16) throw JetError{JET_ERR_OVERFLOW, "connectivity table update exceeded its bounds"};
+        best.cut = c.best_cut;
+        best.total_imb = c.best_imb;
+        curr.cut = c.curr_cut;
+        curr.total_imb = c.curr_imb;
+        total_iters += c.iter_count;
+    }
+
     // jet_refine, src/jet_refiner.hpp:1050-1142.  best_part in/out.
     jet_level_stats_c refine(const Level<O, E, W>& L, part_t* best_part, double imb, double tol, bool ultra) {
         auto t0 = clk::now();
@@ -380,6 +573,20 @@ struct Refiner {
         if (ultra) { for (double t = 0.85; t > 0; t -= 0.05) temps.push_back(t); }
         else if (L.uniform) temps.push_back(0.25);
         else temps.push_back(0.75);
+        if (cta_eligible(L) || use_graph) {
+            if (cta_eligible(L)) run_level_cta(L, best_part, pb, temps, tol);
+            else run_level_graph(L, best_part, pb, temps, tol);
+            jet_level_stats_c cl;
+            cl.edge_cut = (int64_t)(best.cut / 2);
+            cl.imb = (double)best.total_imb / (double)pb.opt;
+            cl.num_edges = (uint64_t)L.m;
+            cl.num_vertices = (uint64_t)L.n;
+            cl.total_ref_time = since(t0);
+            cl.iterations_time = since(t1);
+            cl.total_iterations = hctl->iter_count;
+            cl.lp_iterations = hctl->lab_counter;
+            return cl;
+        }
         int iter_count = 0, balance_counter = 0, lab_counter = 0;
         for (double fr : temps) {
             int count = 0;
