@@ -54,7 +54,11 @@ EXPORTED_SYMBOLS = [
     "jet_partition_i32", "jet_partition_big", "jet_partition_biggest", "jet_coarsen_map", "jet_contract",
     "jet_conn_build", "jet_refine_iters", "jet_refine_level", "jet_pstat", "jet_project", "jet_version",
     "jet_last_error", "jet_device_ok", "jet_prof_enable", "jet_prof_read", "jet_launch_count", "jet_pstat_noalloc",
+    "jet_set_refine_drivers",
 ]
+
+# level-loop drivers (jet_set_refine_drivers)
+DRIVER_CTA, DRIVER_COOP, DRIVER_GRAPH, DRIVER_ALL = 1, 2, 4, 7
 
 
 class JetError(RuntimeError):
@@ -107,6 +111,8 @@ def load(build_if_missing: bool = False):
     lib.jet_version.restype = ctypes.c_char_p
     lib.jet_last_error.restype = ctypes.c_char_p
     lib.jet_launch_count.restype = ctypes.c_int64
+    lib.jet_set_refine_drivers.restype = ctypes.c_int
+    lib.jet_set_refine_drivers.argtypes = [ctypes.c_int]
     _lib = lib
     return lib
 
@@ -438,6 +444,12 @@ def project(cmap: torch.Tensor, coarse_part: torch.Tensor, tier: str = "i32") ->
 def launch_count() -> int:
     """Kernels launched by the library so far in this process."""
     return int(load().jet_launch_count())
+
+
+def set_refine_drivers(mask: int) -> int:
+    """Allowed level-loop drivers (DRIVER_* bits); returns the previous mask.
+    Every driver yields the same partition, only the speed differs."""
+    return int(load().jet_set_refine_drivers(int(mask)))
 
 
 def prof_enable(on: bool = True):

@@ -111,7 +111,7 @@ int partition_impl(const jet_config_c* cfg, O n, const E* row, const O* adj, con
         double t_load = since(t0);
         validate<O, E, W>(eng, n, in.m, in.prow, in.padj, in.pval, in.pvw);
         double t_transfer = since(t0);
-        if (getenv("JET_DEBUG_TIMING")) fprintf(stderr, "jet: load %.3f ms validate %.3f ms\n", t_load * 1e3, (t_transfer - t_load) * 1e3);
+        if (debug_timing()) fprintf(stderr, "jet: load %.3f ms validate %.3f ms\n", t_load * 1e3, (t_transfer - t_load) * 1e3);
         if (n == 0) { *cut_out = 0; return JET_OK; }
         DBuf<part_t> part_dev;
         part_t* pout = part_out;

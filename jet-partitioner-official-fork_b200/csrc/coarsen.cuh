@@ -7,6 +7,7 @@
 // HUB_DEG are skipped by group kernels and handled by one CTA each.
 #pragma once
 #include "graph.cuh"
+#include "sort.cuh"
 
 namespace jetb {
 
@@ -222,13 +223,19 @@ __device__ __forceinline__ void atomic_min_o(int32_t* p, int32_t v) { atomicMin(
 template <class O>
 __device__ __forceinline__ void atomic_min_o(int64_t* p, int64_t v) { atomicMin((long long*)p, (long long)v); }
 
+// has_free[u]: bit 0 = u has a free child; bit 1 = u's walk step was claimed.
+// A vertex is stepped through exactly once: either its own thread finds
+// cnt == 0 or its last child continues into it, and both happen only after
+// every child finished; the claim bit keeps the second arrival out.
 template <class O>
 __global__ void k_hec_p2_walk(O n, const O* hn, const uint8_t* inB, O* cnt, O* min_free, int* has_free) {
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < n; x += (int64_t)gridDim.x * blockDim.x) {
         O cur = (O)x;
-        if (!inB[cur] || ld_cg(&cnt[cur]) != 0) continue;  // only leaves start a walk
+        if (!inB[cur] || ld_cg(&cnt[cur]) != 0) continue;  // children pending: the last one continues here
         while (true) {
-            bool is_free = ld_cg(&has_free[cur]) == 0;
+            if (atomicOr(&has_free[cur], 2) & 2) break;  // already stepped through
+            __threadfence();
+            bool is_free = (ld_cg(&has_free[cur]) & 1) == 0;
             O v = hn[cur];
             if (!inB[v]) break;
             if (is_free) {
@@ -249,7 +256,7 @@ __global__ void k_hec_p2_roots(O n, const O* hn, const uint8_t* inB, const O* mi
         O u = (O)x;
         if (!inB[u]) continue;
         O root;
-        if (has_free[u]) {
+        if (has_free[u] & 1) {
             root = min_free[u];
         } else {
             O v = hn[u];
@@ -549,39 +556,40 @@ __global__ void k_relative_hash(GView<O, E, W> g, const O* list, O cnt, O* hashe
     }
 }
 
-// matchHash, src/heuristics.hpp:277-319: equal digests pair up through an
-// open-addressed table of size `mappable`; probes are bounded.
+// matchHash, src/heuristics.hpp:277-319, in list order: vertices with equal
+// digests pair up consecutively (1st with 2nd, 3rd with 4th, ...), which is
+// what the reference's table loop gives when run in list order with the
+// entries whose digest equals the table's null key run last (those all share
+// the first free slot past their home slot).  On the device: a stable radix
+// sort by digest, then group ranks from a scan of group heads.
 template <class O, class H>
-__global__ void k_match_hash(const O* list, const H* hashes, O mappable, H nullkey, H* htable, O* twins, O* vcmap, int* err) {
-    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < mappable; x += (int64_t)gridDim.x * blockDim.x) {
-        O i = list[x];
-        H h = hashes[x];
-        O key = (O)(h % (H)mappable);
-        int64_t guard = 0;
-        bool found = false;
-        while (!found) {
-            if (ld_cg(&htable[key]) == nullkey) atomic_cas(&htable[key], nullkey, h);
-            if (ld_cg(&htable[key]) == h) { found = true; break; }
-            key++;
-            if (key >= mappable) key -= mappable;
-            if (++guard > (int64_t)mappable + 1) { atomicOr(err, ERRF_PROBE); break; }
-        }
-        if (!found) continue;
-        guard = 0;
-        while (true) {
-            O twin = ld_cg(&twins[key]);
-            if (twin == -1) {
-                if (atomic_cas(&twins[key], twin, i) == twin) break;
-            } else {
-                if (atomic_cas(&twins[key], twin, (O)-1) == twin) {
-                    O cv = twin < i ? twin : i;
-                    st_v(&vcmap[twin], cv);
-                    st_v(&vcmap[i], cv);
-                    break;
-                }
-            }
-            if (++guard > (1 << 24)) { atomicOr(err, ERRF_SPIN); break; }
-        }
+struct GetDigestKey {
+    const H* h;
+    H nullkey;
+    H null_as;  // key the null digest sorts under (its own group)
+    __device__ __forceinline__ H operator()(int64_t i) const { H v = h[i]; return v == nullkey ? null_as : v; }
+};
+template <class K, class O>
+struct GetGroupHead {
+    const K* sk;
+    __device__ __forceinline__ O operator()(int64_t q) const { return (q == 0 || sk[q] != sk[q - 1]) ? (O)1 : (O)0; }
+};
+template <class K, class O>
+__global__ void k_group_starts(const K* sk, int64_t n, const O* ex, O* start) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x)
+        if (q == 0 || sk[q] != sk[q - 1]) start[ex[q]] = (O)q;
+}
+template <class K, class O>
+__global__ void k_pair_groups(const K* sk, const O* sx, const O* list, int64_t n, const O* ex, const O* start, O* vcmap) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        bool head = q == 0 || sk[q] != sk[q - 1];
+        O gid = ex[q] + (head ? 1 : 0) - 1;
+        int64_t r = q - (int64_t)start[gid];
+        if ((r & 1) || q + 1 >= n || sk[q + 1] != sk[q]) continue;
+        O a = list[sx[q]], b = list[sx[q + 1]];
+        O cv = a < b ? a : b;
+        vcmap[a] = cv;
+        vcmap[b] = cv;
     }
 }
 

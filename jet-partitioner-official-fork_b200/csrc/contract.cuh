@@ -325,4 +325,58 @@ __global__ void __launch_bounds__(1024) k_contract_copy_hub(const O* list, const
     }
 }
 
+// ---------------------------------------------------------------- hub rows in neighbour order
+// Rows built in the global table (du > 4096) come out in slot order; these
+// put them in neighbour-id order like every other row.  Hub row x (coarse
+// vertex list[x]) owns entries [hoff[x], hoff[x+1]) of the enumeration.
+template <class O, class E>
+struct GetHubRowSize {
+    const O* list;
+    const E* crow;
+    __device__ __forceinline__ E operator()(int64_t x) const { O c = list[x]; return crow[c + 1] - crow[c]; }
+};
+template <class E>
+__device__ __forceinline__ int64_t hub_row_of(const E* hoff, int64_t nhub, int64_t q) {
+    int64_t lo = 0, hi = nhub - 1;  // last x with hoff[x] <= q
+    while (lo < hi) {
+        int64_t mid = (lo + hi + 1) >> 1;
+        if ((int64_t)hoff[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+template <class O, class E>
+struct GetHubKey {
+    const O* list;
+    const E* crow;
+    const E* hoff;
+    int64_t nhub;
+    const O* cadj;
+    int nb;  // bits of a neighbour id
+    __device__ __forceinline__ uint64_t operator()(int64_t q) const {
+        int64_t x = hub_row_of<E>(hoff, nhub, q);
+        E pos = crow[list[x]] + (E)(q - (int64_t)hoff[x]);
+        return ((uint64_t)x << nb) | (uint64_t)cadj[pos];
+    }
+};
+template <class O, class E, class W>
+__global__ void k_hub_gather(const O* list, const E* crow, const E* hoff, int64_t nhub, int64_t total, const int64_t* sq,
+                             const W* cval, W* tval) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t q = sq[t];
+        int64_t x = hub_row_of<E>(hoff, nhub, q);
+        tval[t] = cval[crow[list[x]] + (E)(q - (int64_t)hoff[x])];
+    }
+}
+template <class O, class E, class W>
+__global__ void k_hub_place(const O* list, const E* crow, const E* hoff, int64_t total, const uint64_t* skey,
+                            const W* tval, int nb, O* cadj, W* cval) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t key = skey[t];
+        int64_t x = (int64_t)(key >> nb);
+        E pos = crow[list[x]] + (E)(t - (int64_t)hoff[x]);
+        cadj[pos] = (O)(key & ((1ull << nb) - 1ull));
+        cval[pos] = tval[t];
+    }
+}
+
 }  // namespace jetb

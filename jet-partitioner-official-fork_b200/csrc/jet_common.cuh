@@ -130,6 +130,10 @@ template <class T> __host__ __device__ __forceinline__ T ceil_div(T a, T b) { re
 // code corrects it by the number of times the captured kernels ran.
 void count_launch();
 int64_t launch_counter();
+// Which level-loop drivers refinement may use (JET_DRIVER_* bits).
+int refine_drivers();
+// JET_DEBUG_TIMING set in the environment: phase timings go to stderr.
+bool debug_timing();
 void add_launches(int64_t n);
 // True while this thread captures work into a CUDA graph (profiling event
 // records are skipped: they are not allowed inside conditional bodies).
@@ -146,6 +150,7 @@ void pinned_release(int slot);
 struct Dev {
     int sms = 148;
     int max_smem_optin = 227 * 1024;
+    int coop = 0;  // cooperative launches supported
 };
 Dev& device_info();
 

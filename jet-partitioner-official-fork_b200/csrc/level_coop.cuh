@@ -18,6 +18,7 @@ struct GridBar {
     unsigned int gen;
     int abort;
     int pad;
+    int64_t nmarked;             // rows queued for rebuild this iteration
 };
 
 // Returns false when the loop must stop (a barrier timed out somewhere).
@@ -158,6 +159,7 @@ struct CoopScratch {
     O* sv0;
     O* sv1;
     W* wpre;             // prefix of candidate weights in sorted order (n)
+    O* marked;           // rows to rebuild after a large move set (n)
 };
 
 // Rebalance tail over the grid (sort_candidates + k_evict_sorted [+ strong]).
@@ -279,14 +281,26 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
         }
         d_update_small_hub<true, O, E, W>(a);
         if (!grid_sync(cs.bar, err)) return;
-        d_conn_warp<O, E, W>(a, nullptr, n, 1, &a.dev->large);  // update_large: rebuild marked rows
-        if (!grid_sync(cs.bar, err)) return;
+        if (a.dev->large) {
+            // update_large: queue the marked rows (one coalesced pass), then
+            // rebuild them one warp per row
+            for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+                int64_t i = base + threadIdx.x;
+                bool take = i < n && a.mark[i];
+                int64_t s = warp_append(&cs.bar->nmarked, take);
+                if (take) cs.marked[s] = (O)i;
+            }
+            if (!grid_sync(cs.bar, err)) return;
+            d_conn_warp<O, E, W>(a, cs.marked, (O)((volatile GridBar*)cs.bar)->nmarked, 1, nullptr);
+            if (!grid_sync(cs.bar, err)) return;
+        }
         d_cut_after<O, E, W>(a);
         if (!grid_sync(cs.bar, err)) return;
         if (blockIdx.x == 0) {
             W mx = block_max_sizes<W>(a.sizes, a.k);
             if (threadIdx.x == 0) {
                 ctl_end_logic<O, W>(c, a.dev, mx);
+                cs.bar->nmarked = 0;
                 if (c->more && ++iters >= max_iters) { c->more = 0; atomicOr(err, ERRF_SPIN); }
             }
         }

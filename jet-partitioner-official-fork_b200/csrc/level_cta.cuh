@@ -14,6 +14,7 @@
 namespace jetb {
 
 static constexpr int CTA_MAX_N = 16384;   // candidate sort buffer: CTA_MAX_N x 8 B in shared memory
+static constexpr int64_t CTA_MAX_M = 262144;  // beyond this many entries one SM's bandwidth is the limit
 static constexpr int CTA_MAX_K = 256;     // per-warp connectivity tables: 32 warps x k slots
 static constexpr int CTA_THREADS = 1024;
 

@@ -37,6 +37,7 @@ template <class O, class E, class W>
 struct Engine {
     cudaStream_t s;
     ScanScratch scan;
+    RadixScratch rsort;
     DBuf<int64_t> dscal;   // small device scalars
     int64_t* hscal = nullptr;  // pinned mirror
     IterResult* hres = nullptr;
@@ -216,6 +217,7 @@ struct Engine {
             cur = nxt;
             if (outer > 100000) throw JetError{JET_ERR_TIMEOUT, "matching did not settle"};
         }
+        if (debug_timing()) fprintf(stderr, "jet:   matching n %lld outer %d\n", (long long)n, outer);
         if (two_hop) two_hop_passes(L, vcmap);
         k_singletons<O><<<grid_persistent(n, 16), BLOCK, 0, s>>>(n, vcmap); count_launch();
         JET_LAUNCH_CHECK();
@@ -246,23 +248,28 @@ struct Engine {
         return cnt;
     }
 
+    // matchHash in list order (see k_pair_groups).  The null digest sorts as
+    // `null_as` (a value no other digest takes); keys use `bits` bits.
     template <class H>
-    void match_hash(const O* list, const H* hashes, O mappable, H nullkey, O* vcmap) {
+    void match_hash(const O* list, const H* hashes, O mappable, H nullkey, H null_as, int bits, O* vcmap) {
         if (mappable <= 0) return;
-        DBuf<H> ht(mappable, s);
-        DBuf<O> twins(mappable, s);
-        fill<H>(ht.p, mappable, nullkey, s);
-        fill<O>(twins.p, mappable, (O)-1, s);
-        int* err = dslot<int>(30);
-        JET_CUDA(cudaMemsetAsync(err, 0, sizeof(int64_t), s));
-        k_match_hash<O, H><<<grid_persistent(mappable, 16), BLOCK, 0, s>>>(list, hashes, mappable, nullkey, ht.p, twins.p, vcmap, err); count_launch();
+        DBuf<H> k0(mappable, s), k1(mappable, s);
+        DBuf<O> v0(mappable, s), v1(mappable, s), ex(mappable, s), start(mappable, s);
+        int which = radix_sort_pairs<H, O>(GetDigestKey<O, H>{hashes, nullkey, null_as}, GetIndex<O>{}, (int64_t)mappable, bits,
+                                           k0.p, v0.p, k1.p, v1.p, rsort, scan, s);
+        const H* sk = which == 0 ? k0.p : k1.p;
+        const O* sx = which == 0 ? v0.p : v1.p;
+        exclusive_scan<O, GetGroupHead<H, O>>(GetGroupHead<H, O>{sk}, (int64_t)mappable, ex.p, nullptr, scan, s);
+        k_group_starts<H, O><<<grid_persistent(mappable, 16), BLOCK, 0, s>>>(sk, (int64_t)mappable, ex.p, start.p); count_launch();
+        k_pair_groups<H, O><<<grid_persistent(mappable, 16), BLOCK, 0, s>>>(sk, sx, list, (int64_t)mappable, ex.p, start.p, vcmap); count_launch();
         JET_LAUNCH_CHECK();
-        JET_CUDA(cudaMemcpyAsync(hscal, err, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-        sync();
-        if (*(int*)hscal) throw JetError{JET_ERR_TIMEOUT, "2-hop hash matching exceeded its probe bound"};
     }
 
     void two_hop_passes(Level<O, E, W>& L, O* vcmap) {
+        struct Report {
+            clk::time_point t;
+            ~Report() { if (debug_timing()) fprintf(stderr, "jet:   two-hop %.3f ms\n", since(t) * 1e3); }
+        } rep{clk::now()};
         auto g = L.view();
         O n = L.n;
         const O MAXV = ord_max<O>();
@@ -274,7 +281,7 @@ struct Engine {
                 DBuf<O> hs(cnt, s);
                 k_leaf_hash<O, E, W><<<grid_persistent(cnt, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p); count_launch();
                 JET_LAUNCH_CHECK();
-                match_hash<O>(list.p, hs.p, cnt, MAXV, vcmap);
+                match_hash<O>(list.p, hs.p, cnt, MAXV, n, bits_for((uint64_t)n), vcmap);
             }
         }
         unmapped = count_unmatched(n, vcmap);
@@ -289,7 +296,7 @@ struct Engine {
                     k_twin_hash_hub<O, E, W><<<grid_for(cnt, 1) < 4096 ? grid_for(cnt, 1) : 4096, 1024, 0, s>>>(g, list.p, cnt, hs.p); count_launch();
                     JET_LAUNCH_CHECK();
                 }
-                match_hash<uint64_t>(list.p, hs.p, cnt, (uint64_t)0, vcmap);
+                match_hash<uint64_t>(list.p, hs.p, cnt, (uint64_t)0, (uint64_t)0, 64, vcmap);
             }
         }
         unmapped = count_unmatched(n, vcmap);
@@ -300,7 +307,7 @@ struct Engine {
                 DBuf<O> hs(cnt, s);
                 k_relative_hash<O, E, W><<<grid_persistent(cnt, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p); count_launch();
                 JET_LAUNCH_CHECK();
-                match_hash<O>(list.p, hs.p, cnt, MAXV, vcmap);
+                match_hash<O>(list.p, hs.p, cnt, MAXV, n, bits_for((uint64_t)n), vcmap);
             }
         }
     }
@@ -309,6 +316,32 @@ struct Engine {
     O coarsen_map(Level<O, E, W>& L, int alg, uint64_t seed, int level, O* vcmap, O* hn_out, double* meas) {
         if (alg == 1) return hec_map(L, seed, level, vcmap, hn_out, meas ? &meas[M_HEAVY] : nullptr, meas ? &meas[M_MAPCONSTRUCT] : nullptr);
         return match_map(L, alg == 0, seed, level, vcmap, hn_out);
+    }
+
+    // Puts the hub rows of C (coarse vertices list[0..nhub)) in neighbour order:
+    // one stable radix sort of (row rank, neighbour id) keys over their entries.
+    void sort_hub_rows(const O* list, int64_t nhub, O nc, Level<O, E, W>& C) {
+        DBuf<E> hoff(nhub + 1, s);
+        E* tot = dslot<E>(45);
+        exclusive_scan<E, GetHubRowSize<O, E>>(GetHubRowSize<O, E>{list, C.own_row.p}, nhub, hoff.p, tot, scan, s);
+        JET_CUDA(cudaMemcpyAsync(&hscal[5], tot, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        sync();
+        int64_t total = (int64_t)*(E*)&hscal[5];
+        if (total <= 1) return;
+        int nb = bits_for((uint64_t)nc);
+        int bits = nb + bits_for((uint64_t)nhub);
+        if (bits > 64) throw JetError{JET_ERR_INVALID, "hub row sort key exceeds 64 bits"};
+        DBuf<uint64_t> k0(total, s), k1(total, s);
+        DBuf<int64_t> v0(total, s), v1(total, s);
+        DBuf<W> tval(total, s);
+        int which = radix_sort_pairs<uint64_t, int64_t>(GetHubKey<O, E>{list, C.own_row.p, hoff.p, nhub, C.own_adj.p, nb},
+                                                        GetIndex<int64_t>{}, total, bits, k0.p, v0.p, k1.p, v1.p, rsort, scan, s);
+        const uint64_t* sk = which == 0 ? k0.p : k1.p;
+        const int64_t* sq = which == 0 ? v0.p : v1.p;
+        unsigned grid = grid_persistent(total, 16);
+        k_hub_gather<O, E, W><<<grid, BLOCK, 0, s>>>(list, C.own_row.p, hoff.p, nhub, total, sq, C.own_val.p, tval.p); count_launch();
+        k_hub_place<O, E, W><<<grid, BLOCK, 0, s>>>(list, C.own_row.p, hoff.p, total, sk, tval.p, nb, C.own_adj.p, C.own_val.p); count_launch();
+        JET_LAUNCH_CHECK();
     }
 
     // ------------------------------------------------------------ contraction
@@ -373,6 +406,8 @@ struct Engine {
         JET_LAUNCH_CHECK();
         k_contract_copy_hub<O, E, W><<<device_info().sms, 1024, 0, s>>>(lh.p, nh, hrow.p, skey, sval, C.own_row.p, C.own_adj.p, C.own_val.p); count_launch();
         JET_LAUNCH_CHECK();
+        int64_t nhub = (int64_t)*(O*)&hscal[2];
+        if (nhub > 0) sort_hub_rows(lh.p, nhub, nc, C);
         C.row = C.own_row.p;
         C.adj = C.own_adj.p;
         C.val = C.own_val.p;

@@ -21,6 +21,7 @@ Dev& device_info() {
         if (cudaGetDeviceProperties(&p, dev) == cudaSuccess) {
             d.sms = p.multiProcessorCount;
             d.max_smem_optin = (int)p.sharedMemPerBlockOptin;
+            d.coop = p.cooperativeLaunch;
         }
         cached_dev = dev;
     }
@@ -58,6 +59,12 @@ cudaStream_t default_stream() {
 static std::atomic<int64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 int64_t launch_counter() { return g_launches.load(); }
+static std::atomic<int> g_drivers{JET_DRIVER_ALL};
+int refine_drivers() { return g_drivers.load(); }
+bool debug_timing() {
+    static const bool on = getenv("JET_DEBUG_TIMING") != nullptr;
+    return on;
+}
 void add_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 bool& capturing() {
@@ -223,6 +230,8 @@ int jet_project(int tier, int64_t n_fine, const void* map, const int32_t* coarse
 }
 
 int64_t jet_launch_count(void) { return g_launches.load(); }
+
+int jet_set_refine_drivers(int mask) { return g_drivers.exchange(mask & JET_DRIVER_ALL); }
 
 int jet_prof_enable(int on) {
     prof_collect();

@@ -4,7 +4,7 @@
 #pragma once
 #include "partitioner.cuh"
 #include "sort.cuh"
-#include "level_cta.cuh"
+#include "level_coop.cuh"
 
 namespace jetb {
 
@@ -33,6 +33,11 @@ struct Refiner {
     bool verbose = false;
     bool use_graph = true;
     bool use_cta = true;
+    bool use_coop = true;
+    DBuf<GridBar> cbar;
+    DBuf<W> cwsum;
+    DBuf<uint32_t> chist;
+    DBuf<O> cmarked;
 
     struct HostState {
         W cut = 0;
@@ -65,6 +70,10 @@ struct Refiner {
         dev.zero();
         ctl.alloc(1, s);
         ctl.zero();
+        int drv = refine_drivers();
+        use_cta = (drv & JET_DRIVER_CTA) != 0;
+        use_coop = (drv & JET_DRIVER_COOP) != 0;
+        use_graph = (drv & JET_DRIVER_GRAPH) != 0;
         pslot = pinned_acquire(sizeof(Ctl<W>));
         hctl = (Ctl<W>*)pinned_ptr(pslot);
         std::memset(hctl, 0, sizeof(Ctl<W>));
@@ -410,7 +419,9 @@ struct Refiner {
     }
 
     // ------------------------------------------------------------ single-CTA loop
-    bool cta_eligible(const Level<O, E, W>& L) const { return use_cta && L.n <= CTA_MAX_N && k <= CTA_MAX_K; }
+    bool cta_eligible(const Level<O, E, W>& L) const {
+        return use_cta && L.n <= CTA_MAX_N && (int64_t)L.m <= CTA_MAX_M && k <= CTA_MAX_K;
+    }
 
     void ctl_init(const Prob& pb, const std::vector<double>& temps, double tol) {
         Ctl<W>& c = *hctl;
@@ -426,7 +437,9 @@ struct Refiner {
         JET_CUDA(cudaMemcpyAsync(hctl, ctl.p, sizeof(Ctl<W>), cudaMemcpyDeviceToHost, s));
         JET_CUDA(cudaMemcpyAsync(e.hres, &dev.p->err, sizeof(int), cudaMemcpyDeviceToHost, s));
         e.sync();
-        if (*(int*)e.hres & ~16) throw JetError{JET_ERR_OVERFLOW, "refinement exceeded a device bound"};
+        int err = *(int*)e.hres;
+        if (err & ERRF_SPIN) throw JetError{JET_ERR_TIMEOUT, "a bounded device loop or grid barrier gave up"};
+        if (err & ~16) throw JetError{JET_ERR_OVERFLOW, "refinement exceeded a device bound"};
         Ctl<W>& c = *hctl;
         best.cut = c.best_cut;
         best.total_imb = c.best_imb;
@@ -447,6 +460,58 @@ struct Refiner {
         k_level_cta<O, E, W><<<1, CTA_THREADS, smem, s>>>(args(L), li, rbw, rbs, ctl.p, best_part, sizes_best.p, P, 1 << 22);
         count_launch();
         JET_LAUNCH_CHECK();
+        ctl_finish();
+    }
+
+    // ------------------------------------------------------------ cooperative loop
+    static constexpr int64_t COOP_MAX_N = (int64_t)1 << 17;  // above this the multi-kernel graph is faster
+    size_t coop_smem() const {
+        int kw = k < WARP_TABLE ? k : WARP_TABLE;
+        size_t nw = CTA_THREADS / 32;
+        size_t conn = ((nw * kw * sizeof(part_t) + 15) & ~(size_t)15) + nw * kw * sizeof(W);
+        size_t rs = (size_t)32 * RS_BINS * sizeof(uint32_t);
+        return (conn > rs ? conn : rs) + 64;
+    }
+    size_t coop_static_smem() const {
+        static size_t bytes = [] {
+            cudaFuncAttributes fa;
+            return cudaFuncGetAttributes(&fa, k_level_coop<O, E, W>) == cudaSuccess ? fa.sharedSizeBytes : (size_t)1 << 30;
+        }();
+        return bytes;
+    }
+    bool coop_eligible(const Level<O, E, W>& L) const {
+        return use_coop && device_info().coop && !cta_eligible(L) && (int64_t)L.n <= COOP_MAX_N && k <= WARP_TABLE &&
+               coop_smem() + coop_static_smem() <= (size_t)device_info().max_smem_optin;
+    }
+
+    // The whole level loop as one cooperative launch (one 1024-thread CTA per
+    // SM); phases meet at bounded grid barriers.
+    void run_level_coop(const Level<O, E, W>& L, part_t* best_part, const Prob& pb, const std::vector<double>& temps, double tol) {
+        size_t smem = coop_smem();
+        JET_CUDA(cudaFuncSetAttribute(k_level_coop<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int per_sm = 0;
+        JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_level_coop<O, E, W>, CTA_THREADS, smem));
+        if (per_sm < 1) throw JetError{JET_ERR_CUDA, "cooperative level kernel does not fit on an SM"};
+        int grid = device_info().sms * per_sm;
+        if (cbar.n < 1) cbar.alloc(1, s);
+        if (cwsum.n < grid) cwsum.alloc(grid, s);
+        if (chist.n < (int64_t)grid * RS_BINS) chist.alloc((int64_t)grid * RS_BINS, s);
+        if (cmarked.n < (int64_t)n_max) cmarked.alloc(n_max > 0 ? n_max : 1, s);
+        JET_CUDA(cudaMemsetAsync(cbar.p, 0, sizeof(GridBar), s));
+        ctl_init(pb, temps, tol);
+        LevelLists<O> li{L.warp_list.p, L.n_warp, L.hub_list.p, L.n_hub, L.group};
+        RebArgs<O, W> rbw = reb_args(L, weak_max_dest(pb.size_max), pb.opt, pb.size_max, false);
+        RebArgs<O, W> rbs = reb_args(L, strong_max_dest(pb.opt, pb.size_max), pb.opt, pb.size_max, false);
+        CoopScratch<O, E, W> cs{cbar.p, cwsum.p, chist.p, sk0.p, sk1.p, sv0.p, sv1.p, wpre.p, cmarked.p};
+        int bits = bits_for((uint64_t)rbw.none_key);
+        int max_iters = 1 << 22;
+        RefArgs<O, E, W> a = args(L);
+        Ctl<W>* cp = ctl.p;
+        part_t* bp = best_part;
+        W* sb = sizes_best.p;
+        void* params[] = {&a, &li, &rbw, &rbs, &cp, &bp, &sb, &cs, &bits, &max_iters};
+        JET_CUDA(cudaLaunchCooperativeKernel((const void*)k_level_coop<O, E, W>, dim3(grid), dim3(CTA_THREADS), params, smem, s));
+        count_launch();
         ctl_finish();
     }
 
@@ -573,8 +638,9 @@ struct Refiner {
         if (ultra) { for (double t = 0.85; t > 0; t -= 0.05) temps.push_back(t); }
         else if (L.uniform) temps.push_back(0.25);
         else temps.push_back(0.75);
-        if (cta_eligible(L) || use_graph) {
+        if (cta_eligible(L) || coop_eligible(L) || use_graph) {
             if (cta_eligible(L)) run_level_cta(L, best_part, pb, temps, tol);
+            else if (coop_eligible(L)) run_level_coop(L, best_part, pb, temps, tol);
             else run_level_graph(L, best_part, pb, temps, tol);
             jet_level_stats_c cl;
             cl.edge_cut = (int64_t)(best.cut / 2);
@@ -695,6 +761,9 @@ W run_partition(Engine<O, E, W>& eng, const Cfg& cfg, const GraphIn<O, E, W>& in
         O nc = eng.coarsen_map(cur, alg, seed, (int)levels.size(), map.p, nullptr, meas);
         prof_end(h, PK_HEC, 0, s);
         meas[M_MAP] += since(tm);
+        if (debug_timing())
+            fprintf(stderr, "jet: level %d n %lld m %lld map %.3f ms nc %lld\n", (int)levels.size(), (long long)cur.n,
+                    (long long)cur.m, since(tm) * 1e3, (long long)nc);
         if (nc < min_allowed) break;
         auto tb = clk::now();
         std::unique_ptr<Level<O, E, W>> next(new Level<O, E, W>());

@@ -26,6 +26,9 @@
 //     emits hash-slot order, src/contract.hpp:320-327).
 //   * rebalance_weak with no undersized part leaves the vertex in place (the
 //     reference divides by zero there, src/jet_refiner.hpp:618).
+//   * matchHash (src/heuristics.hpp:277-319) runs the entries whose digest
+//     equals the table's null key after all others, so each digest value
+//     pairs its members consecutively in list order.
 // Reference files are cited as path:line inside the reference project.
 
 #include <cstdint>
@@ -244,9 +247,15 @@ void match_hash(const std::vector<O>& list, const std::vector<H>& hashes, H null
     if (mappable == 0) return;
     std::vector<H> htable(mappable, nullkey);
     std::vector<O> twins(mappable, -1);
+    // List order, except that entries whose digest equals the null key run
+    // after all others (one of the orders the reference's parallel loop can
+    // take): they then all meet in one free slot, so every digest value forms
+    // its own group and members pair up consecutively.
+    for (int pass = 0; pass < 2; pass++)
     for (O x = 0; x < mappable; x++) {
         O i = list[x];
         H h = hashes[x];
+        if ((h == nullkey) != (pass == 1)) continue;
         O key = (O)(h % (H)mappable);
         while (true) {
             if (htable[key] == nullkey) htable[key] = h;

@@ -55,9 +55,9 @@ def test_contract_bit_exact(jet, graphs, orc, tier, kind):
     assert got.nnz == len(want.adj)
     assert np.array_equal(host(got.row), want.row)
     assert np.array_equal(host(got.vw), want.vw)
-    ga, gv = sorted_rows(host(got.row), host(got.adj), host(got.val))
-    assert np.array_equal(ga, want.adj)
-    assert np.array_equal(gv, want.val)
+    # every row, hub rows included, comes out in neighbour order
+    assert np.array_equal(host(got.adj), want.adj)
+    assert np.array_equal(host(got.val), want.val)
 
 
 @pytest.mark.parametrize("tier", TIERS)
@@ -98,9 +98,10 @@ def test_match_proposals_bit_exact(jet, graphs, orc, kind, uniform):
 
 @pytest.mark.parametrize("tier", TIERS)
 @pytest.mark.parametrize("kind", ["grid2d", "grid3d", "rgg", "rmat", "star"])
-@pytest.mark.parametrize("alg,uniform", [(1, True), (1, False), (2, True), (2, False)])
+@pytest.mark.parametrize("alg,uniform", [(1, True), (1, False), (2, True), (2, False), (0, True), (0, False)])
 def test_coarsen_map_bit_exact(jet, graphs, orc, tier, kind, alg, uniform):
-    """HEC and pure matching produce the oracle's (in-order) map exactly."""
+    """HEC, pure matching and 2-hop matching produce the oracle's (in-order)
+    map exactly."""
     g = make(graphs, kind, tier)
     og = orc.G.from_csr(g)
     m, nc, _ = orc.coarsen(og, alg, level=2, seed=13, uniform=uniform)
@@ -191,10 +192,11 @@ def test_rebalance_iterations_bit_exact(jet, graphs, orc, tier, kind, k):
 
 @pytest.mark.parametrize("tier", TIERS)
 @pytest.mark.parametrize("kind,alg,k", [("grid2d", 1, 16), ("grid3d", 1, 32), ("rgg", 1, 8), ("rgg", 2, 16),
-                                        ("grid2d", 2, 8)])
+                                        ("grid2d", 2, 8), ("rmat", 0, 16), ("star", 0, 8), ("rmat", 1, 32)])
 def test_full_partition_bit_exact(jet, graphs, orc, tier, kind, alg, k):
-    """HEC and pure matching: the whole multilevel run (coarsening, Metis,
-    refinement, projection) returns the oracle's partition for the same seed."""
+    """HEC, pure and 2-hop matching: the whole multilevel run (coarsening,
+    Metis, refinement, projection) returns the oracle's partition for the
+    same seed."""
     g = make(graphs, kind, tier)
     og = orc.G.from_csr(g)
     for seed in (1, 2):
@@ -287,3 +289,48 @@ def test_edge_cases(jet, graphs, orc):
     p = host(part)
     assert p.min() >= 0 and p.max() < 3
     assert orc.pstat(orc.G.from_csr(small), p, 3)[0] == cut
+
+
+@pytest.mark.parametrize("drivers", ["all", "no_cta", "graph", "host"])
+@pytest.mark.parametrize("tier,kind,k", [("i32", "grid2d", 16), ("big", "rgg", 64), ("biggest", "grid2d", 300),
+                                         ("i32", "rgg", 600)])
+def test_level_drivers_bit_exact(jet, graphs, orc, drivers, tier, kind, k):
+    """Every level-loop driver (one CTA, cooperative grid kernel, CUDA graph
+    with conditional nodes, host loop) returns the oracle's partition on
+    graphs whose finer levels exceed the one-CTA bound."""
+    mask = {"all": jet.DRIVER_ALL, "no_cta": jet.DRIVER_COOP | jet.DRIVER_GRAPH, "graph": jet.DRIVER_GRAPH,
+            "host": 0}[drivers]
+    g = graphs.grid2d(170, 150, weighted=True, seed=7) if kind == "grid2d" else graphs.rgg(30000, 9.0, seed=5)
+    g = g.as_tier(tier)
+    og = orc.G.from_csr(g)
+    want, wcut, _ = orc.partition(og, k, alg=1, imb=1.03, seed=3)
+    prev = jet.set_refine_drivers(mask)
+    try:
+        cfg = jet.config_t(coarsening_alg=1, num_parts=k, max_imb_ratio=1.03)
+        fn = {"i32": jet.partition, "big": jet.partition_big, "biggest": jet.partition_biggest}[tier]
+        part, cut, _ = fn(cfg, g.to("cuda"), seed=3)
+    finally:
+        jet.set_refine_drivers(prev)
+    assert cut == wcut
+    assert np.array_equal(host(part), want)
+
+
+@pytest.mark.parametrize("wl", ["grid3d128_k64", "rmat16_k64_2hop"])
+def test_full_size_partition_bit_exact(jet, graphs, orc, wl):
+    """Large inputs (2M-vertex mesh; 2^16-vertex R-MAT with 2-hop matching):
+    the large-level paths drive every fine level and the result is still the
+    oracle's partition, run after run."""
+    if wl == "grid3d128_k64":
+        g = graphs.grid3d(128, 128, 128, weighted=True, seed=1)
+        k, alg, imb, fn = 64, 1, 1.03, jet.partition
+    else:
+        g = graphs.rmat(16, 8, seed=1, tier="big")
+        k, alg, imb, fn = 64, 0, 1.10, jet.partition_big
+    og = orc.G.from_csr(g)
+    want, wcut, _ = orc.partition(og, k, alg=alg, imb=imb, seed=1)
+    cfg = jet.config_t(coarsening_alg=alg, num_parts=k, max_imb_ratio=imb)
+    gd = g.to("cuda")
+    for _ in range(2):
+        part, cut, _ = fn(cfg, gd, seed=1)
+        assert cut == wcut
+        assert np.array_equal(host(part), want)
