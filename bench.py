@@ -149,6 +149,49 @@ def run_reference(args, wl, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_only(args, wl, local):
+    """Connectivity-table build (init_conn_data) alone on the finest graph
+    with a fixed random k-way partition: the library's CUDA events around the
+    table-build kernels of each call, inputs resident, L2 flushed between
+    calls."""
+    import torch
+
+    torch.cuda.set_device(local)
+    jet = load_pkg()
+    dev = torch.device("cuda", local)
+    g = wl["make"](jet.graphs, dev)
+    k = wl["k"]
+    gen = torch.Generator(device=dev).manual_seed(1)
+    part = torch.randint(0, k, (g.n,), generator=gen, device=dev, dtype=torch.int32)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        jet.conn_build(g, part, k)
+    times, nbytes, slots = [], 0.0, 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        # the library's own CUDA events bracket exactly the table-build kernels
+        jet.prof_enable(True)
+        off, ent, val, size = jet.conn_build(g, part, k)
+        prof = jet.prof_read()["conn_build"]
+        jet.prof_enable(False)
+        times.append(prof["ms"])
+        nbytes = prof["bytes"]
+        slots = int(off[-1].item())
+    ms = statistics.median(times)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = nbytes / (ms / 1000.0) / 1e9
+    print(json.dumps({"kernel": "conn_build", "workload": args.workload, "n": g.n, "nnz": g.nnz, "k": k, "slots": slots,
+                      "ms_median": ms, "algorithmic_bytes": nbytes, "achieved_gbs": achieved, "peak_gbs": peak,
+                      "frac": achieved / peak, "steps": args.steps}), flush=True)
+
+
 def config_of(args, wl, g):
     return {"workload": args.workload, "graph": wl["desc"], "n": g.n, "undirected_edges": g.nnz // 2, "k": wl["k"],
             "coarsening": ALG_NAME[wl["alg"]], "imbalance": wl["imb"], "tier": wl["tier"],
@@ -164,11 +207,16 @@ def main():
     ap.add_argument("--workload", default="grid3d128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--only", default=None, choices=["conn_build"],
+                    help="time one kernel alone on the workload's finest graph (profiling case)")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_env()
     if args.impl == "reference":
         run_reference(args, wl, rank)
+        return
+    if args.only:
+        run_only(args, wl, local)
         return
 
     import torch

@@ -33,18 +33,24 @@ inline cudaStream_t pick_stream(void* s) { return s ? (cudaStream_t)s : default_
 // Rejects graphs the refinement cannot handle: non-monotone offsets, neighbour
 // ids out of range, non-positive vertex or edge weights (a zero vertex weight
 // would make gain_bucket divide by zero and never terminate).
+// Vertices and entries are checked in two flat passes, so hub rows cost no
+// more than any other entries.
 template <class O, class E, class W>
 __global__ void k_validate(O n, E m, const E* row, const O* adj, const W* val, const W* vw, int* err) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int bad = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
         E a = row[i], b = row[i + 1];
-        if (b < a || a < 0 || b > m) { atomicOr(err, 1); continue; }
-        if (vw[i] <= 0) atomicOr(err, 4);
-        for (E j = a; j < b; j++) {
-            O v = adj[j];
-            if (v < 0 || v >= n) { atomicOr(err, 2); break; }
-            if (val[j] <= 0) { atomicOr(err, 8); break; }
-        }
+        if (b < a || a < 0 || b > m) bad |= 1;
+        if (vw[i] <= 0) bad |= 4;
     }
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < (int64_t)m; j += stride) {
+        O v = adj[j];
+        if (v < 0 || v >= n) bad |= 2;
+        if (val[j] <= 0) bad |= 8;
+    }
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0 && bad) atomicOr(err, bad);
     if (blockIdx.x == 0 && threadIdx.x == 0 && (row[0] != 0 || row[n] != m)) atomicOr(err, 1);
 }
 
@@ -52,7 +58,7 @@ template <class O, class E, class W>
 void validate(Engine<O, E, W>& eng, O n, E m, const E* row, const O* adj, const W* val, const W* vw) {
     int* err = eng.template dslot<int>(60);
     JET_CUDA(cudaMemsetAsync(err, 0, sizeof(int64_t), eng.s));
-    k_validate<O, E, W><<<grid_persistent(n > 0 ? n : 1, 8), BLOCK, 0, eng.s>>>(n, m, row, adj, val, vw, err); count_launch();
+    k_validate<O, E, W><<<grid_persistent((int64_t)m + n + 1, 8), BLOCK, 0, eng.s>>>(n, m, row, adj, val, vw, err); count_launch();
     JET_LAUNCH_CHECK();
     JET_CUDA(cudaMemcpyAsync(&eng.hscal[0], err, sizeof(int64_t), cudaMemcpyDeviceToHost, eng.s));
     eng.sync();

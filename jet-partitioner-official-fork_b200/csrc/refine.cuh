@@ -86,25 +86,12 @@ struct RefArgs {
 };
 
 // ---------------------------------------------------------------- table build
-// Writes a final table of `size` slots into the vertex's region from a list of
-// (part, weight) pairs held by the caller; region must be cleared first.
-template <class W>
-__device__ __forceinline__ bool table_put_private(Slot<W>* base, part_t size, part_t k, part_t p, W w) {
-    part_t po = p % size;
-    if (size < k) {
-        part_t guard = 0;
-        while (base[po].p != NULL_PART) {
-            po = (po + 1) % size;
-            if (++guard > size) return false;
-        }
-    }
-    base[po].p = p;
-    base[po].v = w;
-    return true;
-}
-
 // deg <= 32: one thread per vertex, its distinct parts gathered in a private
 // 32-entry shared-memory set (interleaved so threads hit distinct banks).
+// Neighbours are read in batches of 8 with every load issued before the first
+// use, so a row costs about two memory latencies instead of two per entry.
+// The final table (at most 32 slots) is laid out with a register bitmask of
+// occupied slots and written once, with no read-back.
 template <class O, class E, class W>
 __global__ void __launch_bounds__(128) k_conn_thread(RefArgs<O, E, W> a, int only_marked, const int* gate) {
     __shared__ part_t sk[32][128];
@@ -117,27 +104,60 @@ __global__ void __launch_bounds__(128) k_conn_thread(RefArgs<O, E, W> a, int onl
         E deg = re - rs;
         if (deg > THREAD_DEG) continue;
         if (only_marked && !a.mark[i]) continue;
-        for (int s = 0; s < (int)deg; s++) sk[s][t] = NULL_PART;
+        const int sz = (int)deg;  // set capacity: at most deg distinct parts
+        for (int s = 0; s < sz; s++) sk[s][t] = NULL_PART;
         int used = 0;
-        int sz = (int)deg;  // set capacity: at most deg distinct parts
         bool ok = true;
-        for (E j = rs; j < re; j++) {
-            part_t p = a.part[a.g.adj[j]];
-            W w = a.g.val[j];
-            int h = p % sz;
-            int guard = 0;
-            while (sk[h][t] != NULL_PART && sk[h][t] != p && ++guard <= sz) h = h + 1 == sz ? 0 : h + 1;
-            if (guard > sz) { ok = false; break; }
-            if (sk[h][t] == NULL_PART) { sk[h][t] = p; sv[h][t] = w; used++; }
-            else sv[h][t] += w;
+        for (E j0 = rs; j0 < re; j0 += 8) {
+            O vb[8];
+            W wb[8];
+            part_t pb[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) vb[u] = j0 + u < re ? a.g.adj[j0 + u] : (O)0;
+#pragma unroll
+            for (int u = 0; u < 8; u++) wb[u] = j0 + u < re ? a.g.val[j0 + u] : (W)0;
+#pragma unroll
+            for (int u = 0; u < 8; u++) pb[u] = j0 + u < re ? a.part[vb[u]] : NULL_PART;
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                part_t p = pb[u];
+                if (p == NULL_PART || !ok) continue;
+                int h = p % sz;
+                int guard = 0;
+                while (sk[h][t] != NULL_PART && sk[h][t] != p && ++guard <= sz) h = h + 1 == sz ? 0 : h + 1;
+                if (guard > sz) { ok = false; continue; }
+                if (sk[h][t] == NULL_PART) { sk[h][t] = p; sv[h][t] = wb[u]; used++; }
+                else sv[h][t] += wb[u];
+            }
         }
         part_t cap = conn_cap<E>(deg, a.k);
         part_t size = cap == 0 ? 0 : shrunk_size(used, cap);
         Slot<W>* base = a.slots + a.coff[i];
-        for (int s = 0; s < cap; s++) { base[s].p = NULL_PART; base[s].v = 0; }
+        uint32_t occ = 0;  // size <= cap <= 32
         for (int s = 0; ok && s < sz; s++) {
             part_t p = sk[s][t];
-            if (p != NULL_PART) ok = table_put_private<W>(base, size, a.k, p, sv[s][t]);
+            if (p == NULL_PART) continue;
+            int po = p % size;
+            if (size < a.k) {
+                int guard = 0;
+                while ((occ >> po) & 1u) {
+                    po = po + 1 == size ? 0 : po + 1;
+                    if (++guard > size) { ok = false; break; }
+                }
+                if (!ok) break;
+            }
+            occ |= 1u << po;
+            Slot<W> sl;
+            sl.p = p;
+            sl.v = sv[s][t];
+            base[po] = sl;
+        }
+        for (int s = 0; s < cap; s++) {
+            if ((occ >> s) & 1u) continue;
+            Slot<W> sl;
+            sl.p = NULL_PART;
+            sl.v = 0;
+            base[s] = sl;
         }
         if (!ok) atomicOr(&a.dev->err, ERRF_OVERFLOW);
         a.csize[i] = size;
