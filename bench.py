@@ -21,6 +21,7 @@ from __future__ import annotations
 import argparse
 import importlib.util
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -192,6 +193,119 @@ def run_only(args, wl, local):
                       "frac": achieved / peak, "steps": args.steps}), flush=True)
 
 
+def batched_workload(jet, dev, count, seed=0):
+    """512 random geometric graphs in the unit square (the batched config):
+    n log-uniform in [1e3, 2e5], radius for mean degree 10, edge weights
+    uniform in [1, 10], k uniform over {8, 16, 32, 64}, imbalance 1.03, HEC."""
+    import random
+    rng = random.Random(seed)
+    gs, cfgs, seeds = [], [], []
+    for i in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(1e3), math.log(2e5)))))
+        k = rng.choice([8, 16, 32, 64])
+        gs.append(jet.graphs.rgg(n, 10.0, seed=i, device=dev))
+        cfgs.append(jet.config_t(coarsening_alg=1, num_parts=k, max_imb_ratio=1.03))
+        seeds.append(i + 1)
+    return gs, cfgs, seeds
+
+
+def run_batched(jet, dev, count, workers):
+    """Plain (one graph per call, one after another) against the batched
+    executor on the same graphs; wall clock with the device synchronised on
+    both sides (the batched run spans many streams)."""
+    import torch
+    gs, cfgs, seeds = batched_workload(jet, dev, count)
+    for g, c, s in list(zip(gs, cfgs, seeds))[:3]:
+        jet.partition(c, g, seed=s)
+    jet.partition_batch(cfgs[:workers], gs[:workers], seeds[:workers], workers=workers)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = [jet.partition(c, g, seed=s)[1] for g, c, s in zip(gs, cfgs, seeds)]
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    res = jet.partition_batch(cfgs, gs, seeds, workers=workers)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    lat = sorted(r[2] for r in res)
+    edges = sum(g.nnz for g in gs) // 2
+    return {"graphs": count, "workers": workers, "sum_vertices": sum(g.n for g in gs), "sum_undirected_edges": edges,
+            "plain_graphs_per_s": count / t_plain, "batched_graphs_per_s": count / t_batch,
+            "speedup": t_plain / t_batch, "batched_edges_per_s": edges / t_batch,
+            "equal_cut": all(r[1] == p for r, p in zip(res, plain)),
+            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "timing": "wall clock, device synchronised before and after"}
+
+
+def serving_workload(jet, dev, count, seed=5):
+    """Requests mixing 2D grids, random geometric graphs and R-MAT graphs:
+    n log-uniform in [1e4, 1e6], mean degree in [6, 16], k in {16..256}."""
+    import random
+    rng = random.Random(seed)
+    reqs = []
+    for i in range(count):
+        n = int(round(math.exp(rng.uniform(math.log(1e4), math.log(1e6)))))
+        kind = rng.choice(["grid", "rgg", "rmat"])
+        k = rng.choice([16, 32, 64, 128, 256])
+        deg = rng.uniform(6, 16)
+        if kind == "grid":
+            side = max(8, int(math.sqrt(n)))
+            g = jet.graphs.grid2d(side, max(8, n // side), weighted=True, seed=i, device=dev)
+            cfg = jet.config_t(coarsening_alg=1, num_parts=k, max_imb_ratio=1.03)
+        elif kind == "rgg":
+            g = jet.graphs.rgg(n, deg, seed=i, device=dev)
+            cfg = jet.config_t(coarsening_alg=1, num_parts=k, max_imb_ratio=1.03)
+        else:
+            scale = max(10, int(round(math.log2(n))))
+            g = jet.graphs.rmat(scale, max(2, int(deg / 2)), seed=i, tier="i32", device=dev)
+            cfg = jet.config_t(coarsening_alg=0, num_parts=k, max_imb_ratio=1.10)
+        reqs.append((cfg, g, i + 1))
+    return reqs
+
+
+def run_serving(jet, dev, count, workers, budget):
+    """A request stream through the server: first all at once (capacity),
+    then Poisson arrivals at 1.2x and 0.5x that capacity; latency is submit
+    to result."""
+    import random
+    import torch
+    reqs = serving_workload(jet, dev, count)
+    torch.cuda.synchronize()
+    out = {"requests": count, "workers": workers, "budget_bytes": budget}
+
+    def stream(rate):
+        srv = jet.Server("i32", workers=workers, mem_budget_bytes=budget)
+        rng = random.Random(11)
+        t0 = time.perf_counter()
+        tickets = []
+        next_t = 0.0
+        for cfg, g, sd in reqs:
+            if rate:
+                next_t += rng.expovariate(rate)
+                d = t0 + next_t - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+            tickets.append(srv.submit(cfg, g, seed=sd))
+        res = [srv.wait(t) for t in tickets]
+        dt = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        lat = sorted(r[2] for r in res)
+        return {"graphs_per_s": len(res) / dt, "p50_ms": lat[len(lat) // 2],
+                "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))], "peak_concurrent": st["peak_concurrent"],
+                "peak_footprint_bytes": st["peak_footprint_bytes"], "failed": st["failed"]}, res
+
+    cap, res0 = stream(None)
+    out["all_at_once"] = cap
+    out["poisson_1.2x"], res1 = stream(1.2 * cap["graphs_per_s"])
+    out["poisson_0.5x"], _ = stream(0.5 * cap["graphs_per_s"])
+    cfg, g, sd = reqs[0]
+    alone = jet.partition(cfg, g, seed=sd)
+    out["same_alone_and_in_mix"] = bool(alone[1] == res0[0][1] == res1[0][1] and
+                                        torch.equal(alone[0], res0[0][0]) and torch.equal(alone[0], res1[0][0]))
+    return out
+
+
 def config_of(args, wl, g):
     return {"workload": args.workload, "graph": wl["desc"], "n": g.n, "undirected_edges": g.nnz // 2, "k": wl["k"],
             "coarsening": ALG_NAME[wl["alg"]], "imbalance": wl["imb"], "tier": wl["tier"],
@@ -207,6 +321,9 @@ def main():
     ap.add_argument("--workload", default="grid3d128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--batched", type=int, default=512, help="graphs in the batched comparison (0 = skip)")
+    ap.add_argument("--serving", type=int, default=96, help="requests in the serving run (0 = skip)")
+    ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--only", default=None, choices=["conn_build"],
                     help="time one kernel alone on the workload's finest graph (profiling case)")
     args = ap.parse_args()
@@ -219,6 +336,9 @@ def main():
         run_only(args, wl, local)
         return
 
+    # separate hardware queues for the batched executor's worker streams
+    # (read when the CUDA context is created)
+    os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
     import torch
     import torch.distributed as dist
     from datetime import timedelta
@@ -287,6 +407,8 @@ def main():
     h2d = (g.n + 1) * eb + g.nnz * (ob + wb) + g.n * wb
     d2h = g.n * 4
     e2e_value = ws * len(e2e_times) / sum(e2e_times) if e2e_times else None
+    batched = run_batched(jet, dev, args.batched, args.workers) if args.batched > 0 else None
+    serving = run_serving(jet, dev, args.serving, args.workers, 120 << 30) if args.serving > 0 else None
 
     if rank != 0:
         if ws > 1:
@@ -329,6 +451,8 @@ def main():
         "roofline": roof,
         "kernel_classes_ms": {nm: round(v["ms"], 3) for nm, v in prof.items()},
         "cpu_baseline": cpu_base,
+        "batched": batched,
+        "serving": serving,
         "clocks": clk,
         "gpu_launches": launches,
     }

@@ -98,6 +98,69 @@ int jet_partition_biggest(const jet_config_c* config, int64_t n, const int64_t* 
                           const int64_t* values, const int64_t* vweights, int uniform_ew, int mem, uint64_t seed,
                           void* stream, int32_t* part_out, int64_t* edge_cut, jet_stats_c* stats);
 
+/* ---------------------------------------------------------------- batched
+ * Many graphs of one tier in one call (no counterpart in the reference,
+ * which partitions one graph per call).  Each graph is an independent
+ * partition with the same result as the single-graph entry point given the
+ * same arguments; `workers` host threads (0 = 8) each drive their own CUDA
+ * stream on the current device and pull the next graph (largest nnz first),
+ * so kernels of different graphs overlap on the GPU and the host-side Metis
+ * calls overlap GPU work (they run in helper processes, because Metis keeps
+ * global state).  Workers use the one-CTA level loop and the host loop only.
+ * Set CUDA_DEVICE_MAX_CONNECTIONS=32 in the environment before the process
+ * creates its CUDA context so that the workers' streams get separate
+ * hardware queues.  Array
+ * element types follow the tier as in jet_partition_*; `mem` applies to all
+ * graphs.  Returns JET_OK when every graph succeeded, else the first failing
+ * graph's code (each graph's own code is in its `status`). */
+typedef struct jet_graph_desc {
+    int64_t n;
+    const void* row_map;
+    const void* entries;
+    const void* values;
+    const void* vweights;
+    int32_t uniform_ew;
+    jet_config_c config;
+    uint64_t seed;
+    int32_t* part_out;     /* n entries (memory kind as `mem`) */
+    int64_t edge_cut;      /* out: the cut, each edge once */
+    int32_t status;        /* out: JET_OK or an error code */
+    double latency_ms;     /* out: from submission (batch start) to completion */
+    char error[112];       /* out: message when status != JET_OK */
+} jet_graph_desc;
+
+int jet_partition_batch(int tier, int64_t count, jet_graph_desc* graphs, int mem, int workers);
+
+/* ---------------------------------------------------------------- serving
+ * A request loop over the batched executor: requests are queued as they
+ * arrive and admitted (oldest first) while a worker is free and the sum of
+ * the admitted requests' estimated device footprints stays within
+ * `mem_budget_bytes`; admitted requests run concurrently on their own
+ * streams.  A request whose estimate alone exceeds the budget is refused
+ * with JET_ERR_OOM.  The caller keeps a request's arrays alive until its
+ * ticket is waited for.  Results equal those of jet_partition_* for the same
+ * arguments, alone or in any mix.  (No counterpart in the reference.) */
+typedef struct jet_server jet_server;
+typedef struct jet_server_stats {
+    int64_t submitted, completed, failed, refused;
+    int64_t peak_footprint_bytes;   /* largest admitted sum seen */
+    int32_t peak_concurrent;        /* most requests in flight at once */
+} jet_server_stats;
+
+jet_server* jet_server_create(int tier, int mem, int workers, int64_t mem_budget_bytes);
+/* Queues a copy of *req; returns a ticket >= 0, or -(error code). */
+int64_t jet_server_submit(jet_server* srv, const jet_graph_desc* req);
+/* Waits up to timeout_ms (< 0: forever) for a ticket.  JET_OK once the
+ * request has finished: *out holds it with its outputs and its own result
+ * code in out->status, and the ticket is released.  JET_ERR_TIMEOUT when it
+ * is not done yet (wait again); JET_ERR_INVALID for an unknown ticket. */
+int jet_server_wait(jet_server* srv, int64_t ticket, jet_graph_desc* out, double timeout_ms);
+/* Estimated device bytes a request holds while it runs (the admission unit). */
+int64_t jet_server_footprint(int tier, int64_t n, int64_t nnz, int32_t num_parts);
+int jet_server_stats_get(jet_server* srv, jet_server_stats* out);
+/* Finishes every queued request, then frees the server. */
+int jet_server_destroy(jet_server* srv);
+
 /* ---------------------------------------------------------------- components
  * Tier-generic entry points over device pointers (tier 0 = i32, 1 = big,
  * 2 = biggest; pointer element types follow the tier).  They expose the hot
@@ -113,8 +176,9 @@ int jet_coarsen_map(int tier, int alg, int level, uint64_t seed, int64_t n, int6
                     void* hn_out, int64_t* nc, void* stream);
 
 /* Contraction under a given map (src/contract.hpp:347-446): crow[nc+1],
- * cadj[>= nnz], cval[>= nnz], cvw[nc]; *cnnz receives the coarse nnz.  Row
- * order within a coarse row is unspecified. */
+ * cadj[>= nnz], cval[>= nnz], cvw[nc]; *cnnz receives the coarse nnz.  Each
+ * coarse row lists its neighbours in increasing id (the reference leaves the
+ * order to its hash slots, src/contract.hpp:320-327). */
 int jet_contract(int tier, int64_t n, int64_t nnz, const void* row_map, const void* entries, const void* values,
                  const void* vweights, const void* map, int64_t nc, void* crow, void* cadj, void* cval, void* cvw,
                  int64_t* cnnz, void* stream);

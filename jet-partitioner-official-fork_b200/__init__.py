@@ -54,7 +54,8 @@ EXPORTED_SYMBOLS = [
     "jet_partition_i32", "jet_partition_big", "jet_partition_biggest", "jet_coarsen_map", "jet_contract",
     "jet_conn_build", "jet_refine_iters", "jet_refine_level", "jet_pstat", "jet_project", "jet_version",
     "jet_last_error", "jet_device_ok", "jet_prof_enable", "jet_prof_read", "jet_launch_count", "jet_pstat_noalloc",
-    "jet_set_refine_drivers",
+    "jet_set_refine_drivers", "jet_partition_batch", "jet_server_create", "jet_server_submit", "jet_server_wait",
+    "jet_server_footprint", "jet_server_stats_get", "jet_server_destroy",
 ]
 
 # level-loop drivers (jet_set_refine_drivers)
@@ -306,6 +307,144 @@ def partition_host_biggest(config, g, vweights=None, uniform_ew=None, seed=1):
 
 
 partition_serial_biggest = partition_host_biggest
+
+
+# ------------------------------------------------------------------ batched and served
+class jet_graph_desc(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("row_map", ctypes.c_void_p), ("entries", ctypes.c_void_p),
+                ("values", ctypes.c_void_p), ("vweights", ctypes.c_void_p), ("uniform_ew", ctypes.c_int32),
+                ("config", jet_config_c), ("seed", ctypes.c_uint64), ("part_out", ctypes.c_void_p),
+                ("edge_cut", ctypes.c_int64), ("status", ctypes.c_int32), ("latency_ms", ctypes.c_double),
+                ("error", ctypes.c_char * 112)]
+
+
+class jet_server_stats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("refused", ctypes.c_int64), ("peak_footprint_bytes", ctypes.c_int64),
+                ("peak_concurrent", ctypes.c_int32)]
+
+
+def _desc(tier: str, config: config_t, g: CSRGraph, seed: int, keep: list) -> jet_graph_desc:
+    """Fills a request for one graph; tensors it points at are appended to
+    `keep` (they must outlive the call or the request)."""
+    o, e, w = TIERS[tier]
+    row = g.row.to(e).contiguous()
+    adj = g.adj.to(o).contiguous()
+    val = g.val.to(w).contiguous()
+    vw = g.vw.to(w).contiguous()
+    part = torch.empty(g.n, dtype=torch.int32, device=row.device)
+    keep.append((row, adj, val, vw, part))
+    d = jet_graph_desc()
+    d.n = g.n
+    d.row_map, d.entries, d.values, d.vweights = row.data_ptr(), adj.data_ptr(), val.data_ptr(), vw.data_ptr()
+    d.uniform_ew = int(bool(g.uniform))
+    d.config = config.to_c()
+    d.seed = seed
+    d.part_out = part.data_ptr()
+    return d
+
+
+def partition_batch(configs, graphs, seeds=None, workers: int = 8, tier: str = "i32"):
+    """Partitions many graphs of one tier in one call (jet_partition_batch).
+    `configs` is one config_t or one per graph.  All graphs on the GPU or
+    all on the host.  Returns [(part, edge_cut, latency_ms)], each result
+    equal to the single-graph call with the same config and seed."""
+    _require_cuda()
+    lib = load()
+    graphs = list(graphs)
+    if not graphs:
+        return []
+    if isinstance(configs, config_t):
+        configs = [configs] * len(graphs)
+    seeds = list(seeds) if seeds is not None else [1] * len(graphs)
+    on_dev = graphs[0].row.is_cuda
+    if any(g.row.is_cuda != on_dev for g in graphs):
+        raise JetError(JET_ERR_INVALID, "graphs must all be on the GPU or all on the host")
+    keep = []
+    arr = (jet_graph_desc * len(graphs))()
+    for i, (c, g, sd) in enumerate(zip(configs, graphs, seeds)):
+        arr[i] = _desc(tier, c, g, sd, keep)
+    if on_dev:
+        torch.cuda.synchronize()
+    rc = lib.jet_partition_batch(TIER_ID[tier], ctypes.c_int64(len(graphs)), arr,
+                                 JET_MEM_DEVICE if on_dev else JET_MEM_HOST, int(workers))
+    if rc != JET_OK:
+        bad = [i for i in range(len(graphs)) if arr[i].status != JET_OK]
+        raise JetError(rc, "batched partition failed for graphs %s: %s" % (bad[:8], arr[bad[0]].error.decode() if bad else ""))
+    return [(keep[i][4], int(arr[i].edge_cut), float(arr[i].latency_ms)) for i in range(len(graphs))]
+
+
+class Server:
+    """Request loop (jet_server_*): submit() queues a partition request and
+    returns a ticket; requests are admitted oldest first while a worker is
+    free and their estimated device footprints fit the byte budget, and run
+    concurrently.  wait() returns (part, edge_cut, latency_ms)."""
+
+    def __init__(self, tier: str = "i32", workers: int = 8, mem_budget_bytes: int = 120 << 30, device_memory: bool = True):
+        _require_cuda()
+        self._lib = load()
+        self._lib.jet_server_create.restype = ctypes.c_void_p
+        self._lib.jet_server_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int64]
+        self._lib.jet_server_submit.restype = ctypes.c_int64
+        self._lib.jet_server_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(jet_graph_desc)]
+        self._lib.jet_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(jet_graph_desc),
+                                              ctypes.c_double]
+        self._lib.jet_server_stats_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(jet_server_stats)]
+        self._lib.jet_server_destroy.argtypes = [ctypes.c_void_p]
+        self.tier = tier
+        self.device_memory = device_memory
+        self._h = self._lib.jet_server_create(TIER_ID[tier], JET_MEM_DEVICE if device_memory else JET_MEM_HOST,
+                                              int(workers), ctypes.c_int64(int(mem_budget_bytes)))
+        if not self._h:
+            raise JetError(JET_ERR_INVALID, "server creation failed")
+        self._keep = {}
+
+    def submit(self, config: config_t, g: CSRGraph, seed: int = 1) -> int:
+        if self.device_memory and not g.row.is_cuda:
+            raise JetError(JET_ERR_INVALID, "this server takes graphs in GPU memory")
+        keep = []
+        d = _desc(self.tier, config, g, seed, keep)
+        if self.device_memory:
+            torch.cuda.current_stream().synchronize()
+        t = int(self._lib.jet_server_submit(self._h, ctypes.byref(d)))
+        if t < 0:
+            raise JetError(-t, "request refused")
+        self._keep[t] = keep
+        return t
+
+    def wait(self, ticket: int, timeout_ms: float = -1.0):
+        out = jet_graph_desc()
+        rc = self._lib.jet_server_wait(self._h, ctypes.c_int64(ticket), ctypes.byref(out), ctypes.c_double(timeout_ms))
+        if rc == JET_ERR_TIMEOUT:
+            raise TimeoutError(ticket)
+        _check(rc)
+        keep = self._keep.pop(ticket)
+        if out.status != JET_OK:
+            raise JetError(out.status, "request %d failed: %s" % (ticket, out.error.decode()))
+        return keep[0][4], int(out.edge_cut), float(out.latency_ms)
+
+    def stats(self) -> dict:
+        st = jet_server_stats()
+        _check(self._lib.jet_server_stats_get(self._h, ctypes.byref(st)))
+        return {f: getattr(st, f) for f, _ in jet_server_stats._fields_}
+
+    def close(self):
+        if self._h:
+            self._lib.jet_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def server_footprint(tier: str, n: int, nnz: int, k: int) -> int:
+    """Estimated device bytes one request holds while it runs."""
+    lib = load()
+    lib.jet_server_footprint.restype = ctypes.c_int64
+    return int(lib.jet_server_footprint(TIER_ID[tier], ctypes.c_int64(n), ctypes.c_int64(nnz), ctypes.c_int32(k)))
 
 
 # ------------------------------------------------------------------ components

@@ -15,8 +15,9 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libjetb200.so")
+HELPER = os.path.join(HERE, "jet_metis_helper")
 BUILD = os.path.join(HERE, "_build")
-UNITS = ["runtime.cu", "tier_i32.cu", "tier_big.cu", "tier_biggest.cu", "noalloc.cu"]
+UNITS = ["runtime.cu", "tier_i32.cu", "tier_big.cu", "tier_biggest.cu", "noalloc.cu", "batch.cu"]
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 METIS = os.path.join(CUDA, "targets", "x86_64-linux", "lib", "libmetis_static.a")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -24,12 +25,12 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
 
 
 def _sources():
-    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh"))] + \
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".cpp"))] + \
         [os.path.join(HERE, "..", "include", "jet_b200.h")]
 
 
 def up_to_date() -> bool:
-    if not os.path.exists(OUT):
+    if not os.path.exists(OUT) or not os.path.exists(HELPER):
         return False
     t = os.path.getmtime(OUT)
     return all(os.path.getmtime(s) <= t for s in _sources())
@@ -63,6 +64,13 @@ def build(force: bool = False, ptxas_verbose: bool = False) -> str:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("link failed")
     os.replace(tmp, OUT)
+    # helper process for concurrent Metis calls (batched and served modes)
+    cmd = ["g++", "-O2", "-o", HELPER + ".tmp", os.path.join(CSRC, "metis_helper.cpp"), METIS, "-lm"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("metis helper build failed")
+    os.replace(HELPER + ".tmp", HELPER)
     return OUT
 
 

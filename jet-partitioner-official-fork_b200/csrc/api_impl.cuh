@@ -84,7 +84,7 @@ struct Inputs {
         if (mem == JET_MEM_DEVICE) {
             prow = r; padj = a; pval = v; pvw = w;
             JET_CUDA(cudaMemcpyAsync(&m, r + n, sizeof(E), cudaMemcpyDeviceToHost, s));
-            JET_CUDA(cudaStreamSynchronize(s));
+            stream_wait(s);
             return;
         }
         m = r[n];
@@ -254,13 +254,13 @@ struct Tier {
         if (C <= 0) return;
         std::vector<Slot<W>> h(C);
         JET_CUDA(cudaMemcpyAsync(h.data(), slots, sizeof(Slot<W>) * C, cudaMemcpyDeviceToHost, s));
-        JET_CUDA(cudaStreamSynchronize(s));
+        stream_wait(s);
         std::vector<int32_t> he(C);
         std::vector<W> hv(C);
         for (int64_t i = 0; i < C; i++) { he[i] = h[i].p; hv[i] = h[i].v; }
         if (ent) JET_CUDA(cudaMemcpyAsync(ent, he.data(), sizeof(int32_t) * C, cudaMemcpyHostToDevice, s));
         if (val) JET_CUDA(cudaMemcpyAsync(val, hv.data(), sizeof(W) * C, cudaMemcpyHostToDevice, s));
-        JET_CUDA(cudaStreamSynchronize(s));
+        stream_wait(s);
     }
 
     static int conn_build(int64_t n, int64_t m, const void* row, const void* adj, const void* val, const int32_t* part, int32_t k,
@@ -311,7 +311,7 @@ struct Tier {
             if (ent || cval) {
                 E C = 0;
                 JET_CUDA(cudaMemcpyAsync(&C, ref.coff.p + n, sizeof(E), cudaMemcpyDeviceToHost, s));
-                JET_CUDA(cudaStreamSynchronize(s));
+                stream_wait(s);
                 unpack(s, ref.slots.p, (int64_t)C, ent, (W*)cval);
             }
             eng.sync();
@@ -350,7 +350,7 @@ struct Tier {
                 k_project<O><<<grid_persistent(n_fine, 16), BLOCK, 0, s>>>((O)n_fine, (const O*)map, coarse, fine); count_launch();
                 JET_LAUNCH_CHECK();
             }
-            JET_CUDA(cudaStreamSynchronize(s));
+            stream_wait(s);
             return JET_OK;
         });
     }

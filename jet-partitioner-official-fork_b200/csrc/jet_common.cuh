@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -134,6 +135,20 @@ int64_t launch_counter();
 int refine_drivers();
 // JET_DEBUG_TIMING set in the environment: phase timings go to stderr.
 bool debug_timing();
+// Largest dynamic shared memory a launch of `func` can request on the
+// current device (opt-in maximum minus the kernel's static shared memory).
+int max_dynamic_smem(const void* func);
+// METIS_PartGraphKway with int64 arrays.  Metis keeps global random state,
+// so concurrent in-process calls would change each other's results: a
+// thread in batch mode sends its call to a helper process (one graph per
+// helper at a time); other threads call in process, one at a time.
+int metis_kway(int64_t n, int64_t m, int64_t* xadj, int64_t* adj, int64_t* vw, int64_t* ew, int64_t nparts, float ub,
+               int64_t* obj, int64_t* part);
+// Waits for a stream; batch-mode threads block on an event instead of
+// spinning, leaving the host cores to the other workers and Metis helpers.
+void stream_wait(cudaStream_t s);
+// True on a batch or server worker thread.
+bool batch_thread();
 void add_launches(int64_t n);
 // True while this thread captures work into a CUDA graph (profiling event
 // records are skipped: they are not allowed inside conditional bodies).

@@ -11,12 +11,6 @@
 #include "refine.cuh"
 #include "../../include/jet_b200.h"
 
-typedef int64_t metis_idx_t;
-typedef float metis_real_t;
-// Public METIS 5 API (this build's library uses 64-bit idx_t, float real_t).
-extern "C" int METIS_PartGraphKway(metis_idx_t*, metis_idx_t*, metis_idx_t*, metis_idx_t*, metis_idx_t*, metis_idx_t*,
-                                   metis_idx_t*, metis_idx_t*, metis_real_t*, metis_real_t*, metis_idx_t*, metis_idx_t*,
-                                   metis_idx_t*);
 
 namespace jetb {
 
@@ -54,7 +48,7 @@ struct Engine {
         pinned_release(slot0);
     }
     template <class T> T* dslot(int i) { return (T*)(dscal.p + i); }
-    void sync() { JET_CUDA(cudaStreamSynchronize(s)); }
+    void sync() { stream_wait(s); }
     // copies `cnt` device scalars starting at slot 0 to the host mirror
     void pull(int cnt) {
         JET_CUDA(cudaMemcpyAsync(hscal, dscal.p, sizeof(int64_t) * cnt, cudaMemcpyDeviceToHost, s));

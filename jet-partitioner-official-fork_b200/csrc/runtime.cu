@@ -3,9 +3,24 @@
 // profiling and the tier-generic C entry points.
 #include "api_impl.cuh"
 #include <atomic>
+#include <condition_variable>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
+#include <dlfcn.h>
+#include <spawn.h>
+#include <signal.h>
+#include <sys/socket.h>
+#include <sys/wait.h>
+#include <unistd.h>
+
+extern char** environ;
+typedef int64_t metis_idx_t;
+typedef float metis_real_t;
+extern "C" int METIS_PartGraphKway(metis_idx_t*, metis_idx_t*, metis_idx_t*, metis_idx_t*, metis_idx_t*, metis_idx_t*,
+                                   metis_idx_t*, metis_idx_t*, metis_real_t*, metis_real_t*, metis_idx_t*, metis_idx_t*,
+                                   metis_idx_t*);
 
 namespace jetb {
 
@@ -60,23 +75,177 @@ static std::atomic<int64_t> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 int64_t launch_counter() { return g_launches.load(); }
 static std::atomic<int> g_drivers{JET_DRIVER_ALL};
-int refine_drivers() { return g_drivers.load(); }
+static thread_local int t_driver_mask = JET_DRIVER_ALL;
+int refine_drivers() { return g_drivers.load() & t_driver_mask; }
 bool debug_timing() {
     static const bool on = getenv("JET_DEBUG_TIMING") != nullptr;
     return on;
 }
 void add_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+int max_dynamic_smem(const void* func) {
+    cudaFuncAttributes fa;
+    JET_CUDA(cudaFuncGetAttributes(&fa, func));
+    return device_info().max_smem_optin - (int)fa.sharedSizeBytes;
+}
+
+// ---------------------------------------------------------------- Metis
+static std::mutex g_metis_inproc;
+static thread_local bool t_batch = false;
+bool batch_thread() { return t_batch; }
+
+namespace {
+struct Helper {
+    pid_t pid = -1;
+    int fd = -1;
+    bool busy = false;
+};
+std::mutex g_hmu;
+std::condition_variable g_hcv;
+std::vector<Helper> g_helpers;
+bool g_helpers_broken = false;
+
+std::string helper_path() {
+    Dl_info info;
+    if (!dladdr((void*)&helper_path, &info) || !info.dli_fname) return "";
+    std::string so = info.dli_fname;
+    size_t slash = so.rfind('/');
+    return (slash == std::string::npos ? std::string(".") : so.substr(0, slash)) + "/jet_metis_helper";
+}
+
+bool spawn_helper(Helper& h) {
+    static const std::string path = helper_path();
+    if (path.empty() || access(path.c_str(), X_OK) != 0) return false;
+    int sv[2];
+    if (socketpair(AF_UNIX, SOCK_STREAM | SOCK_CLOEXEC, 0, sv) != 0) return false;
+    posix_spawn_file_actions_t fa;
+    posix_spawn_file_actions_init(&fa);
+    posix_spawn_file_actions_adddup2(&fa, sv[1], 0);
+    posix_spawn_file_actions_adddup2(&fa, sv[1], 1);
+    char* argv[] = {(char*)path.c_str(), nullptr};
+    pid_t pid = -1;
+    int rc = posix_spawn(&pid, path.c_str(), &fa, nullptr, argv, environ);
+    posix_spawn_file_actions_destroy(&fa);
+    close(sv[1]);
+    if (rc != 0) { close(sv[0]); return false; }
+    h.pid = pid;
+    h.fd = sv[0];
+    return true;
+}
+
+bool send_all(int fd, const void* p, size_t bytes) {
+    const char* c = (const char*)p;
+    while (bytes > 0) {
+        ssize_t r = send(fd, c, bytes, MSG_NOSIGNAL);
+        if (r <= 0) return false;
+        c += r;
+        bytes -= (size_t)r;
+    }
+    return true;
+}
+
+bool recv_all(int fd, void* p, size_t bytes) {
+    char* c = (char*)p;
+    while (bytes > 0) {
+        ssize_t r = recv(fd, c, bytes, 0);
+        if (r <= 0) return false;
+        c += r;
+        bytes -= (size_t)r;
+    }
+    return true;
+}
+
+// Index of a helper now marked busy (its socket in *fd), or -1 when none can
+// be had.
+int acquire_helper(int* fd) {
+    std::unique_lock<std::mutex> lk(g_hmu);
+    size_t cap = std::thread::hardware_concurrency();
+    if (cap < 1) cap = 1;
+    if (cap > 32) cap = 32;
+    while (true) {
+        if (g_helpers_broken) return -1;
+        for (size_t i = 0; i < g_helpers.size(); i++)
+            if (!g_helpers[i].busy && g_helpers[i].fd >= 0) {
+                g_helpers[i].busy = true;
+                *fd = g_helpers[i].fd;
+                return (int)i;
+            }
+        if (g_helpers.size() < cap) {
+            Helper h;
+            if (!spawn_helper(h)) { g_helpers_broken = true; return -1; }
+            h.busy = true;
+            *fd = h.fd;
+            g_helpers.push_back(h);
+            return (int)g_helpers.size() - 1;
+        }
+        g_hcv.wait(lk);
+    }
+}
+
+void release_helper(int i, bool ok) {
+    std::lock_guard<std::mutex> lk(g_hmu);
+    Helper& h = g_helpers[i];
+    if (!ok) {
+        close(h.fd);
+        h.fd = -1;
+        if (h.pid > 0) { kill(h.pid, SIGKILL); waitpid(h.pid, nullptr, 0); }
+        h.pid = -1;
+        g_helpers_broken = true;  // fall back to in-process calls from now on
+    }
+    h.busy = false;
+    g_hcv.notify_one();
+}
+}  // namespace
+
+int metis_kway(int64_t n, int64_t m, int64_t* xadj, int64_t* adj, int64_t* vw, int64_t* ew, int64_t nparts, float ub,
+               int64_t* obj, int64_t* part) {
+    if (t_batch) {
+        int fd = -1;
+        int hi = acquire_helper(&fd);
+        if (hi >= 0) {
+            int64_t hdr[3] = {n, m, nparts};
+            int64_t out[2] = {0, 0};
+            bool ok = send_all(fd, hdr, sizeof(hdr)) && send_all(fd, &ub, sizeof(ub)) &&
+                      send_all(fd, xadj, sizeof(int64_t) * (n + 1)) && send_all(fd, adj, sizeof(int64_t) * m) &&
+                      send_all(fd, vw, sizeof(int64_t) * n) && send_all(fd, ew, sizeof(int64_t) * m) &&
+                      recv_all(fd, out, sizeof(out)) && recv_all(fd, part, sizeof(int64_t) * n);
+            release_helper(hi, ok);
+            if (ok) {
+                *obj = out[1];
+                return (int)out[0];
+            }
+        }
+    }
+    std::lock_guard<std::mutex> lk(g_metis_inproc);
+    metis_idx_t nn = n, ncon = 1, np = nparts;
+    metis_real_t u = ub;
+    return METIS_PartGraphKway(&nn, &ncon, xadj, adj, vw, nullptr, ew, &np, nullptr, &u, nullptr, obj, part);
+}
+
+void stream_wait(cudaStream_t s) {
+    if (!t_batch) {
+        JET_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
+    static thread_local cudaEvent_t ev[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!ev[dev]) JET_CUDA(cudaEventCreateWithFlags(&ev[dev], cudaEventBlockingSync | cudaEventDisableTiming));
+    JET_CUDA(cudaEventRecord(ev[dev], s));
+    JET_CUDA(cudaEventSynchronize(ev[dev]));
+}
+
 bool& capturing() {
     static thread_local bool c = false;
     return c;
 }
 
+// One per thread and device: threads that partition concurrently capture
+// their level graphs independently.
 cudaStream_t capture_stream() {
-    static cudaStream_t streams[64] = {};
+    static thread_local cudaStream_t streams[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    std::lock_guard<std::mutex> lk(g_mu);
     if (!streams[dev]) JET_CUDA(cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking));
     return streams[dev];
 }
@@ -119,10 +288,13 @@ struct ProfState {
     double ms[PK_COUNT] = {0};
     double bytes[PK_COUNT] = {0};
     int64_t launches[PK_COUNT] = {0};
+    int open = 0;  // begun, not yet ended
 };
 static ProfState g_prof;
+static std::recursive_mutex g_prof_mu;  // host threads may partition concurrently
 
 int prof_begin(cudaStream_t s) {
+    std::lock_guard<std::recursive_mutex> lk(g_prof_mu);
     if (!g_prof.on || capturing()) return -1;
     if (g_prof.next + 2 > (int)g_prof.pool.size()) {
         int old = (int)g_prof.pool.size();
@@ -131,17 +303,21 @@ int prof_begin(cudaStream_t s) {
     }
     int h = g_prof.next;
     g_prof.next += 2;
+    g_prof.open++;
     cudaEventRecord(g_prof.pool[h], s);
     return h;
 }
 
 void prof_end(int h, ProfKernel k, double bytes, cudaStream_t s) {
+    std::lock_guard<std::recursive_mutex> lk(g_prof_mu);
     if (h < 0 || !g_prof.on || capturing()) return;
     cudaEventRecord(g_prof.pool[h + 1], s);
     g_prof.pending.push_back({h, (int)k, bytes});
+    g_prof.open--;
 }
 
 void prof_collect() {
+    std::lock_guard<std::recursive_mutex> lk(g_prof_mu);
     if (!g_prof.on) return;
     for (auto& p : g_prof.pending) {
         cudaEventSynchronize(g_prof.pool[p.ev + 1]);
@@ -153,7 +329,7 @@ void prof_collect() {
         }
     }
     g_prof.pending.clear();
-    g_prof.next = 0;
+    if (g_prof.open == 0) g_prof.next = 0;  // events still open elsewhere keep their slots
 }
 
 }  // namespace jetb
@@ -233,8 +409,20 @@ int64_t jet_launch_count(void) { return g_launches.load(); }
 
 int jet_set_refine_drivers(int mask) { return g_drivers.exchange(mask & JET_DRIVER_ALL); }
 
+// Batch and server workers run many partitions side by side.  A cooperative
+// level kernel needs every SM at once and would stall the other streams, and
+// building a level graph costs more host time than its launches save when
+// the GPU is shared, so their threads keep only the one-CTA level loop (the
+// host loop takes the larger levels).  They also wait on streams without
+// spinning and send Metis calls to helper processes.
+void jet_thread_batch_mode(int on) {
+    t_driver_mask = on ? JET_DRIVER_CTA : JET_DRIVER_ALL;
+    t_batch = on != 0;
+}
+
 int jet_prof_enable(int on) {
     prof_collect();
+    std::lock_guard<std::recursive_mutex> lk(g_prof_mu);
     g_prof.on = on != 0;
     for (int i = 0; i < PK_COUNT; i++) { g_prof.ms[i] = 0; g_prof.bytes[i] = 0; g_prof.launches[i] = 0; }
     return JET_OK;

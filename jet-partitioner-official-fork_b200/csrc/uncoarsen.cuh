@@ -456,7 +456,10 @@ struct Refiner {
         int P = 1;
         while (P < (int)L.n) P <<= 1;
         size_t smem = level_cta_smem<O, W>(P, k) + 64;
-        JET_CUDA(cudaFuncSetAttribute(k_level_cta<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // the attribute is per function and process-wide: always the device
+        // maximum, so concurrent callers with different sizes cannot race
+        JET_CUDA(cudaFuncSetAttribute(k_level_cta<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      max_dynamic_smem((const void*)k_level_cta<O, E, W>)));
         k_level_cta<O, E, W><<<1, CTA_THREADS, smem, s>>>(args(L), li, rbw, rbs, ctl.p, best_part, sizes_best.p, P, 1 << 22);
         count_launch();
         JET_LAUNCH_CHECK();
@@ -488,7 +491,8 @@ struct Refiner {
     // SM); phases meet at bounded grid barriers.
     void run_level_coop(const Level<O, E, W>& L, part_t* best_part, const Prob& pb, const std::vector<double>& temps, double tol) {
         size_t smem = coop_smem();
-        JET_CUDA(cudaFuncSetAttribute(k_level_coop<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        JET_CUDA(cudaFuncSetAttribute(k_level_coop<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      max_dynamic_smem((const void*)k_level_coop<O, E, W>)));
         int per_sm = 0;
         JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_level_coop<O, E, W>, CTA_THREADS, smem));
         if (per_sm < 1) throw JetError{JET_ERR_CUDA, "cooperative level kernel does not fit on an SM"};
@@ -707,20 +711,20 @@ void metis_coarsest(const Level<O, E, W>& L, part_t k, double imb, part_t* part_
         JET_CUDA(cudaMemcpyAsync(val.data(), L.val, sizeof(W) * L.m, cudaMemcpyDeviceToHost, s));
     }
     JET_CUDA(cudaMemcpyAsync(vw.data(), L.vw, sizeof(W) * L.n, cudaMemcpyDeviceToHost, s));
-    JET_CUDA(cudaStreamSynchronize(s));
-    metis_idx_t n = L.n, ncon = 1, nparts = k, obj = 0;
-    std::vector<metis_idx_t> xadj(L.n + 1), madj(L.m), madjw(L.m), mvw(L.n), pm(L.n, 0);
+    stream_wait(s);
+    std::vector<int64_t> xadj(L.n + 1), madj(L.m), madjw(L.m), mvw(L.n), pm(L.n > 0 ? L.n : 1, 0);
+    // the reference hands Metis int arrays (src/initial_partition.hpp:65, :103-105)
     for (O i = 0; i <= L.n; i++) xadj[i] = (int)row[i];
     for (E j = 0; j < L.m; j++) { madj[j] = (int)adj[j]; madjw[j] = (int)val[j]; }
     for (O i = 0; i < L.n; i++) mvw[i] = (int)vw[i];
-    metis_real_t ub = (metis_real_t)imb;
-    int ret = METIS_PartGraphKway(&n, &ncon, xadj.data(), madj.data(), mvw.data(), nullptr, madjw.data(), &nparts, nullptr,
-                                  &ub, nullptr, &obj, pm.data());
+    int64_t obj = 0;
+    int ret = metis_kway((int64_t)L.n, (int64_t)L.m, xadj.data(), madj.data(), mvw.data(), madjw.data(), (int64_t)k,
+                         (float)imb, &obj, pm.data());
     if (ret != 1) throw JetError{JET_ERR_METIS, "Metis could not partition coarsest graph"};
     std::vector<part_t> p(L.n);
     for (O i = 0; i < L.n; i++) p[i] = (part_t)pm[i];
     JET_CUDA(cudaMemcpyAsync(part_dev, p.data(), sizeof(part_t) * L.n, cudaMemcpyHostToDevice, s));
-    JET_CUDA(cudaStreamSynchronize(s));
+    stream_wait(s);
 }
 
 struct Cfg {
