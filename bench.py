@@ -54,6 +54,15 @@ WORKLOADS = {
                    k=256, alg=0, imb=1.10, tier="big",
                    make=lambda gr, dev: gr.rmat(18, 8, seed=1, tier="big", device=dev)),
 }
+# DRAM bytes (read + write) per algorithmic byte from one ncu capture of the
+# class's largest launch (profiles/k_conn_thread_grid3d128_k64.md); the
+# per-launch traffic reported is this ratio times the per-launch algorithmic
+# bytes of the timed region.
+NCU_TRAFFIC_RATIO = {
+    "conn_build": {"grid3d128": {"ratio": (126.204928 + 62.770688) / 283.246592,
+                                 "note": "ncu dram bytes of the finest-level launch (189.0 MB of 283.2 MB algorithmic), "
+                                         "scaled to the per-launch average"}},
+}
 ALG_NAME = {0: "2-hop matching", 1: "HEC", 2: "matching"}
 PART_FN = {"i32": "partition", "big": "partition_big", "biggest": "partition_biggest"}
 HOST_FN = {"i32": "partition_host", "big": "partition_host_big", "biggest": "partition_host_biggest"}
@@ -193,48 +202,68 @@ def run_only(args, wl, local):
                       "frac": achieved / peak, "steps": args.steps}), flush=True)
 
 
-def batched_workload(jet, dev, count, seed=0):
-    """512 random geometric graphs in the unit square (the batched config):
-    n log-uniform in [1e3, 2e5], radius for mean degree 10, edge weights
-    uniform in [1, 10], k uniform over {8, 16, 32, 64}, imbalance 1.03, HEC."""
+def batched_specs(count, seed=0):
+    """The batched config: 512 random geometric graphs in the unit square, n
+    log-uniform in [1e3, 2e5], radius for mean degree 10, edge weights
+    uniform in [1, 10], k uniform over {8, 16, 32, 64}, imbalance 1.03, HEC.
+    Returns (n, k) per graph; graph i is generated from seed i."""
     import random
     rng = random.Random(seed)
-    gs, cfgs, seeds = [], [], []
-    for i in range(count):
+    specs = []
+    for _ in range(count):
         n = int(round(math.exp(rng.uniform(math.log(1e3), math.log(2e5)))))
-        k = rng.choice([8, 16, 32, 64])
-        gs.append(jet.graphs.rgg(n, 10.0, seed=i, device=dev))
-        cfgs.append(jet.config_t(coarsening_alg=1, num_parts=k, max_imb_ratio=1.03))
-        seeds.append(i + 1)
-    return gs, cfgs, seeds
+        specs.append((n, rng.choice([8, 16, 32, 64])))
+    return specs
 
 
-def run_batched(jet, dev, count, workers):
+def max_over_ranks(x, ws, dist, device):
+    """Largest value of x over all ranks (x itself when there is one rank)."""
+    if ws <= 1:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None):
     """Plain (one graph per call, one after another) against the batched
     executor on the same graphs; wall clock with the device synchronised on
-    both sides (the batched run spans many streams)."""
+    both sides (the batched run spans many streams).  With several ranks the
+    graphs are sharded by longest-processing-time first and each rank runs
+    its own shard; times are the slowest rank's."""
     import torch
-    gs, cfgs, seeds = batched_workload(jet, dev, count)
+    specs = batched_specs(count)
+    owner = jet.assign_lpt([n for n, _ in specs], ws)
+    mine = [i for i in range(count) if owner[i] == rank]
+    gs = [jet.graphs.rgg(specs[i][0], 10.0, seed=i, device=dev) for i in mine]
+    cfgs = [jet.config_t(coarsening_alg=1, num_parts=specs[i][1], max_imb_ratio=1.03) for i in mine]
+    seeds = [i + 1 for i in mine]
     for g, c, s in list(zip(gs, cfgs, seeds))[:3]:
         jet.partition(c, g, seed=s)
     jet.partition_batch(cfgs[:workers], gs[:workers], seeds[:workers], workers=workers)
     torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
     t0 = time.perf_counter()
     plain = [jet.partition(c, g, seed=s)[1] for g, c, s in zip(gs, cfgs, seeds)]
     torch.cuda.synchronize()
-    t_plain = time.perf_counter() - t0
+    t_plain = max_over_ranks(time.perf_counter() - t0, ws, dist, dev)
+    if ws > 1:
+        dist.barrier()
     t0 = time.perf_counter()
     res = jet.partition_batch(cfgs, gs, seeds, workers=workers)
     torch.cuda.synchronize()
-    t_batch = time.perf_counter() - t0
-    lat = sorted(r[2] for r in res)
+    t_batch = max_over_ranks(time.perf_counter() - t0, ws, dist, dev)
+    equal = max_over_ranks(0.0 if all(r[1] == p for r, p in zip(res, plain)) else 1.0, ws, dist, dev) == 0.0
+    lat = sorted(r[2] for r in res) or [0.0]
     edges = sum(g.nnz for g in gs) // 2
-    return {"graphs": count, "workers": workers, "sum_vertices": sum(g.n for g in gs), "sum_undirected_edges": edges,
+    return {"graphs": count, "graphs_this_rank": len(mine), "workers": workers,
+            "sum_vertices_this_rank": sum(g.n for g in gs), "undirected_edges_this_rank": edges,
             "plain_graphs_per_s": count / t_plain, "batched_graphs_per_s": count / t_batch,
-            "speedup": t_plain / t_batch, "batched_edges_per_s": edges / t_batch,
-            "equal_cut": all(r[1] == p for r, p in zip(res, plain)),
-            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
-            "timing": "wall clock, device synchronised before and after"}
+            "speedup": t_plain / t_batch, "equal_cut": equal,
+            "latency_ms_this_rank": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))]},
+            "timing": "wall clock, device synchronised before and after; max over ranks"}
 
 
 def serving_workload(jet, dev, count, seed=5):
@@ -383,11 +412,9 @@ def main():
     prof = jet.prof_read()
     jet.prof_enable(False)
     total_ms = sum(times)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    max_total_ms = max_over_ranks(total_ms, ws, dist, dev)
     if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    max_total_ms = float(t.item())
     value = ws * args.steps / (max_total_ms / 1000.0)
 
     # end to end through the C ABI with host buffers (copies in the timed region)
@@ -407,8 +434,8 @@ def main():
     h2d = (g.n + 1) * eb + g.nnz * (ob + wb) + g.n * wb
     d2h = g.n * 4
     e2e_value = ws * len(e2e_times) / sum(e2e_times) if e2e_times else None
-    batched = run_batched(jet, dev, args.batched, args.workers) if args.batched > 0 else None
-    serving = run_serving(jet, dev, args.serving, args.workers, 120 << 30) if args.serving > 0 else None
+    batched = run_batched(jet, dev, args.batched, args.workers, ws, rank, dist) if args.batched > 0 else None
+    serving = run_serving(jet, dev, args.serving, args.workers, 120 << 30) if args.serving > 0 and rank == 0 else None
 
     if rank != 0:
         if ws > 1:
@@ -431,7 +458,9 @@ def main():
         per_launch_ms = v["ms"] / v["launches"]
         achieved = (v["bytes"] / v["launches"]) / (per_launch_ms / 1000.0) / 1e9
         roof = {"kernel": nm, "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "peak_source": peak_src,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": NCU_TRAFFIC_RATIO.get(nm, {}).get(args.workload, {}).get("ratio", 0) * v["bytes"] / v["launches"] or None,
+                "traffic_note": NCU_TRAFFIC_RATIO.get(nm, {}).get(args.workload, {}).get("note"),
                 "bytes_per_launch": v["bytes"] / v["launches"], "ms_per_launch": per_launch_ms,
                 "launches": v["launches"]}
     cpu_base = None

@@ -440,6 +440,21 @@ class Server:
             pass
 
 
+def assign_lpt(costs, world_size: int):
+    """Owner rank of each item: longest-processing-time first onto the least
+    loaded rank (ties to the lower rank).  Used to shard independent graphs
+    over GPUs with no collective on the data path."""
+    import heapq
+    world_size = max(1, int(world_size))
+    owner = [0] * len(costs)
+    heap = [(0, r) for r in range(world_size)]
+    for i in sorted(range(len(costs)), key=lambda i: (-costs[i], i)):
+        load, r = heapq.heappop(heap)
+        owner[i] = r
+        heapq.heappush(heap, (load + costs[i], r))
+    return owner
+
+
 def server_footprint(tier: str, n: int, nnz: int, k: int) -> int:
     """Estimated device bytes one request holds while it runs."""
     lib = load()
