@@ -248,15 +248,17 @@ int64_t jet_launch_count(void);
 /* Level-loop drivers refinement may use, process-wide (no counterpart in the
  * reference, whose loop is always host-driven, src/jet_refiner.hpp:1094-1134).
  * Every driver gives identical partitions; the choice only changes speed.
- * A level uses the first allowed of: one CTA (n <= 16384, nnz <= 262144,
- * k <= 256), one cooperative grid kernel (n <= 131072, k <= 512), a CUDA
- * graph with conditional nodes, else the host loop.  Returns the previous
- * mask. */
+ * A level uses the first allowed of: one CTA (n <= 2048, or <= 16384 when
+ * clusters are not allowed; nnz <= 262144; k <= 256), one thread-block
+ * cluster of 8-16 CTAs (n <= 65536, nnz <= 2^21, k <= 512), one cooperative
+ * grid kernel (n <= 131072, nnz <= 2^21, k <= 512), a CUDA graph with
+ * conditional nodes, else the host loop.  Returns the previous mask. */
 enum {
     JET_DRIVER_CTA = 1,
     JET_DRIVER_COOP = 2,
     JET_DRIVER_GRAPH = 4,
-    JET_DRIVER_ALL = 7
+    JET_DRIVER_CLUSTER = 8,
+    JET_DRIVER_ALL = 15
 };
 int jet_set_refine_drivers(int mask);
 

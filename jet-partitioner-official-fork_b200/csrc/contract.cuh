@@ -4,12 +4,13 @@
 // Coarse vertex weights are sums of member weights.  Each coarse row holds
 // the distinct coarse neighbours other than itself with summed edge weights.
 // Work per coarse row c scales with du(c) = sum of member degrees:
-//   du <= 32        one warp per row, dedupe with match.any (rows come out sorted)
-//   32 < du <= 256  128-thread CTA, 512-slot shared-memory hash table
-//   256 < du <= 4K  512-thread CTA, 8192-slot shared-memory hash table
-//   du > 4K         1024-thread CTA, hash table in global scratch (size du)
-// Unique entries land in a scratch array at the row's upper-bound offset,
-// then a copy pass packs them into the coarse CSR.
+//   du <= 32        one warp per row, dedupe with match.any
+//   32 < du <= 256  128-thread CTA, 512-slot shared-memory hash table, sorted
+//   256 < du <= 4K  512-thread CTA, 8192-slot shared-memory hash table, sorted
+//   du > 4K         few coarse ids: a dense shared-memory accumulator per row;
+//                   many: (row, neighbour) keys, a radix sort, reduce-by-key
+// Unique entries land, in neighbour order, in a scratch array at the row's
+// upper-bound offset; a copy pass packs them into the coarse CSR.
 #pragma once
 #include "graph.cuh"
 
@@ -238,43 +239,58 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
     }
 }
 
-// du > 4096: open-addressed table of size du in the row's scratch region.
+// du > 4096 on a level with few coarse vertices: a dense accumulator.  The
+// coarse id range is walked in chunks of `chunk` ids; per chunk the CTA adds
+// every member edge whose coarse neighbour falls in the chunk into a
+// shared-memory array indexed by id, then writes the nonzero entries in id
+// order (edge weights are positive, so a nonzero sum marks a neighbour).
+// Rows come out sorted with no hashing and no sort; the cost is one read of
+// the row's edges per chunk.
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_contract_hub(GView<O, E, W> g, const O* map, const O* list, const O* count,
-                                                       const O* moff, const O* members, const E* hrow, O* skey, W* sval,
-                                                       O* ucnt, int* err) {
+__global__ void __launch_bounds__(1024) k_contract_dense(GView<O, E, W> g, const O* map, const O* list, const O* count,
+                                                         const O* moff, const O* members, const E* hrow, O nc, int chunk,
+                                                         O* skey, W* sval, O* ucnt) {
+    extern __shared__ __align__(16) unsigned char ct_smem[];
+    W* acc = (W*)ct_smem;
     __shared__ E s_pref[1024];
     __shared__ O s_mem[1024];
-    __shared__ unsigned long long s_cnt;
+    __shared__ int s_sw[32];
     O total_rows = *count;
     for (O x = blockIdx.x; x < total_rows; x += gridDim.x) {
         O c = list[x];
-        E hs = hrow[c], d = hrow[c + 1] - hs;
-        for (E s = threadIdx.x; s < d; s += blockDim.x) { skey[hs + s] = (O)-1; sval[hs + s] = 0; }
-        if (threadIdx.x == 0) s_cnt = 0;
-        __syncthreads();
-        cta_for_row_edges<1024>(g, members, moff[c], moff[c + 1], s_pref, s_mem, [&](E j) {
-            O u = map[g.adj[j]];
-            if (u == c) return;
-            W w = g.val[j];
-            E slot = (E)(slot_hash((uint64_t)u) % (uint64_t)d);
-            for (E probe = 0; probe < d; probe++) {
-                O k = ld_cg(&skey[hs + slot]);
-                if (k == (O)-1) {
-                    O old = atomic_cas(&skey[hs + slot], (O)-1, u);
-                    if (old == (O)-1) { atomicAdd(&s_cnt, 1ull); atomic_add(&sval[hs + slot], w); return; }
-                    if (old == u) { atomic_add(&sval[hs + slot], w); return; }
-                } else if (k == u) {
-                    atomic_add(&sval[hs + slot], w);
-                    return;
+        const O m0 = moff[c], m1 = moff[c + 1];
+        E out = hrow[c];
+        for (O base = 0; base < nc; base += chunk) {
+            const O top = nc - base < (O)chunk ? nc : base + chunk;
+            const int len = (int)(top - base);
+            for (int i = threadIdx.x; i < len; i += blockDim.x) acc[i] = 0;
+            __syncthreads();
+            auto add = [&](E j) {
+                O u = map[g.adj[j]];
+                if (u != c && u >= base && u < top) atomic_add(&acc[u - base], g.val[j]);
+            };
+            if (m1 - m0 <= 32) {
+                // few members (the usual case for dense rows): stride over each member's edges
+                for (O mi = m0; mi < m1; mi++) {
+                    O i = members[mi];
+                    for (E j = g.row[i] + threadIdx.x; j < g.row[i + 1]; j += blockDim.x) add(j);
                 }
-                slot++;
-                if (slot >= d) slot = 0;
+            } else {
+                cta_for_row_edges<1024>(g, members, m0, m1, s_pref, s_mem, add);
             }
-            atomicOr(err, ERRF_OVERFLOW);
-        });
-        __syncthreads();
-        if (threadIdx.x == 0) ucnt[c] = (O)s_cnt;
+            __syncthreads();
+            // id-ordered compaction, one 1024-entry tile at a time
+            for (int t0 = 0; t0 < len; t0 += blockDim.x) {
+                int i = t0 + threadIdx.x;
+                W v = i < len ? acc[i] : (W)0;
+                int tot;
+                int ex = block_exclusive_scan<int>(v != 0 ? 1 : 0, s_sw, tot);
+                if (v != 0) { skey[out + ex] = base + (O)i; sval[out + ex] = v; }
+                out += tot;
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) ucnt[c] = (O)(out - hrow[c]);
         __syncthreads();
     }
 }
@@ -288,7 +304,7 @@ __global__ void __launch_bounds__(BLOCK) k_contract_copy(O nc, const E* hrow, co
         if (in) {                                                                           \
             O c = (O)x;                                                                     \
             E hs = hrow[c];                                                                 \
-            if (hrow[c + 1] - hs <= CT_S2_DU) {                                             \
+            {                                                                               \
                 E o = crow[c], cnt = crow[c + 1] - o;                                       \
                 for (E t = lane; t < cnt; t += 32) { cadj[o + t] = skey[hs + t]; cval[o + t] = sval[hs + t]; } \
             }                                                                               \
@@ -298,84 +314,76 @@ __global__ void __launch_bounds__(BLOCK) k_contract_copy(O nc, const E* hrow, co
 #undef CC_BODY
 }
 
+// ---------------------------------------------------------------- hub rows, many coarse ids
+// du > 4096 on a level with many coarse vertices: every hub-row edge becomes
+// a (row rank, coarse neighbour) key, one stable radix sort brings equal keys
+// together in neighbour order, and a reduce-by-key writes each row's unique
+// entries, sorted, into its scratch region.  Work is spread over the whole
+// GPU whatever the row sizes.  hoff[x] is the exclusive prefix of du over
+// the hub list; self-loops and padding get the sentinel key (past every row).
+template <class O, class E>
+struct GetHubDu {
+    const O* list;
+    const E* hrow;
+    __device__ __forceinline__ E operator()(int64_t x) const { O c = list[x]; return hrow[c + 1] - hrow[c]; }
+};
+
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_contract_copy_hub(const O* list, const O* count, const E* hrow, const O* skey,
-                                                            const W* sval, const E* crow, O* cadj, W* cval) {
-    __shared__ unsigned long long s_pos;
+__global__ void __launch_bounds__(1024) k_hub_keys(GView<O, E, W> g, const O* map, const O* list, const O* count,
+                                                   const O* moff, const O* members, const E* hoff, int nb, uint64_t sentinel,
+                                                   uint64_t* key, W* val) {
     O total_rows = *count;
     for (O x = blockIdx.x; x < total_rows; x += gridDim.x) {
         O c = list[x];
-        E hs = hrow[c], d = hrow[c + 1] - hs, o = crow[c];
-        if (threadIdx.x == 0) s_pos = 0;
-        __syncthreads();
-        for (E base = 0; base < d; base += blockDim.x) {
-            E s = base + threadIdx.x;
-            bool occ = s < d && skey[hs + s] != (O)-1;
-            unsigned b = __ballot_sync(0xffffffffu, occ);
-            unsigned long long wpos = 0;
-            if ((threadIdx.x & 31) == 0 && b) wpos = atomicAdd(&s_pos, (unsigned long long)__popc(b));
-            wpos = __shfl_sync(0xffffffffu, wpos, 0);
-            if (occ) {
-                E p = (E)wpos + __popc(b & ((1u << (threadIdx.x & 31)) - 1));
-                cadj[o + p] = skey[hs + s];
-                cval[o + p] = sval[hs + s];
+        E out = hoff[x];
+        for (O mi = moff[c]; mi < moff[c + 1]; mi++) {
+            O i = members[mi];
+            E rs = g.row[i], d = g.row[i + 1] - rs;
+            for (E t = threadIdx.x; t < d; t += blockDim.x) {
+                O u = map[g.adj[rs + t]];
+                key[out + t] = u == c ? sentinel : (((uint64_t)x << nb) | (uint64_t)u);
+                val[out + t] = g.val[rs + t];
             }
+            out += d;
         }
-        __syncthreads();
     }
 }
 
-// ---------------------------------------------------------------- hub rows in neighbour order
-// Rows built in the global table (du > 4096) come out in slot order; these
-// put them in neighbour-id order like every other row.  Hub row x (coarse
-// vertex list[x]) owns entries [hoff[x], hoff[x+1]) of the enumeration.
-template <class O, class E>
-struct GetHubRowSize {
-    const O* list;
-    const E* crow;
-    __device__ __forceinline__ E operator()(int64_t x) const { O c = list[x]; return crow[c + 1] - crow[c]; }
-};
-template <class E>
-__device__ __forceinline__ int64_t hub_row_of(const E* hoff, int64_t nhub, int64_t q) {
-    int64_t lo = 0, hi = nhub - 1;  // last x with hoff[x] <= q
-    while (lo < hi) {
-        int64_t mid = (lo + hi + 1) >> 1;
-        if ((int64_t)hoff[mid] <= q) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-template <class O, class E>
-struct GetHubKey {
-    const O* list;
-    const E* crow;
-    const E* hoff;
-    int64_t nhub;
-    const O* cadj;
-    int nb;  // bits of a neighbour id
-    __device__ __forceinline__ uint64_t operator()(int64_t q) const {
-        int64_t x = hub_row_of<E>(hoff, nhub, q);
-        E pos = crow[list[x]] + (E)(q - (int64_t)hoff[x]);
-        return ((uint64_t)x << nb) | (uint64_t)cadj[pos];
+template <class K, class O>
+struct GetKeyHead {
+    const K* key;
+    K sentinel;
+    __device__ __forceinline__ O operator()(int64_t q) const {
+        K k = key[q];
+        return (k != sentinel && (q == 0 || key[q - 1] != k)) ? (O)1 : (O)0;
     }
 };
-template <class O, class E, class W>
-__global__ void k_hub_gather(const O* list, const E* crow, const E* hoff, int64_t nhub, int64_t total, const int64_t* sq,
-                             const W* cval, W* tval) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-        int64_t q = sq[t];
-        int64_t x = hub_row_of<E>(hoff, nhub, q);
-        tval[t] = cval[crow[list[x]] + (E)(q - (int64_t)hoff[x])];
+
+// First segment index of every row present in the sorted keys.
+static __global__ void k_hub_row_first(const uint64_t* key, int64_t total, int nb, uint64_t sentinel, const int64_t* seg,
+                                int64_t* row_first) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t k = key[q];
+        if (k == sentinel) continue;
+        if (q == 0 || (key[q - 1] >> nb) != (k >> nb)) row_first[k >> nb] = seg[q];
     }
 }
+
 template <class O, class E, class W>
-__global__ void k_hub_place(const O* list, const E* crow, const E* hoff, int64_t total, const uint64_t* skey,
-                            const W* tval, int nb, O* cadj, W* cval) {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-        uint64_t key = skey[t];
-        int64_t x = (int64_t)(key >> nb);
-        E pos = crow[list[x]] + (E)(t - (int64_t)hoff[x]);
-        cadj[pos] = (O)(key & ((1ull << nb) - 1ull));
-        cval[pos] = tval[t];
+__global__ void k_hub_reduce(const uint64_t* key, const W* val, int64_t total, int nb, uint64_t sentinel, const int64_t* seg,
+                             const int64_t* row_first, const O* list, const E* hrow, O* skey, W* sval, O* ucnt) {
+    const uint64_t mask = (1ull << nb) - 1ull;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t k = key[q];
+        if (k == sentinel || (q > 0 && key[q - 1] == k)) continue;
+        W sum = 0;
+        for (int64_t r = q; r < total && key[r] == k; r++) sum += val[r];
+        int64_t x = (int64_t)(k >> nb);
+        O c = list[x];
+        E pos = hrow[c] + (E)(seg[q] - row_first[x]);
+        skey[pos] = (O)(k & mask);
+        sval[pos] = sum;
+        atomic_add(&ucnt[c], (O)1);
     }
 }
 

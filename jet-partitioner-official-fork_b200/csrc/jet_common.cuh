@@ -135,6 +135,8 @@ int64_t launch_counter();
 int refine_drivers();
 // JET_DEBUG_TIMING set in the environment: phase timings go to stderr.
 bool debug_timing();
+// Host clock in milliseconds (steady).
+double host_ms();
 // Largest dynamic shared memory a launch of `func` can request on the
 // current device (opt-in maximum minus the kernel's static shared memory).
 int max_dynamic_smem(const void* func);
@@ -201,31 +203,52 @@ struct Pool {
     int device = -1;
 };
 cudaMemPool_t pool_for_current_device();
+// Large buffers (>= BIG_BYTES) are kept across calls: mapping hundreds of MB
+// into the stream-ordered pool costs milliseconds per allocation.  A block
+// freed on one stream is handed to the next request that fits (within 2x),
+// whose stream first waits for the freeing stream's work.
+static constexpr size_t BIG_BYTES = (size_t)32 << 20;
+void* big_alloc(size_t bytes, cudaStream_t s, size_t* got);
+void big_free(void* p, size_t bytes, cudaStream_t s);
 
 template <class T>
 struct DBuf {
     T* p = nullptr;
     int64_t n = 0;
     cudaStream_t s = nullptr;
+    size_t big = 0;  // bytes of a cached large block (0: from the pool)
     DBuf() {}
     DBuf(int64_t count, cudaStream_t st) { alloc(count, st); }
     void alloc(int64_t count, cudaStream_t st) {
         release();
         s = st;
         n = count;
-        if (count > 0) JET_CUDA(cudaMallocFromPoolAsync((void**)&p, sizeof(T) * (size_t)count, pool_for_current_device(), st));
+        if (count > 0) {
+            size_t bytes = sizeof(T) * (size_t)count;
+            double t0 = debug_timing() ? host_ms() : 0;
+            if (bytes >= BIG_BYTES) p = (T*)big_alloc(bytes, st, &big);
+            else JET_CUDA(cudaMallocFromPoolAsync((void**)&p, bytes, pool_for_current_device(), st));
+            if (debug_timing()) {
+                double dt = host_ms() - t0;
+                if (dt > 1.0) fprintf(stderr, "jet: slow device allocation %.1f MB took %.3f ms\n", bytes / 1e6, dt);
+            }
+        }
     }
     void release() {
-        if (p) cudaFreeAsync(p, s);
+        if (p) {
+            if (big) big_free(p, big, s);
+            else cudaFreeAsync(p, s);
+        }
         p = nullptr;
         n = 0;
+        big = 0;
     }
     ~DBuf() { release(); }
     DBuf(const DBuf&) = delete;
     DBuf& operator=(const DBuf&) = delete;
-    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s), big(o.big) { o.p = nullptr; o.n = 0; o.big = 0; }
     DBuf& operator=(DBuf&& o) noexcept {
-        if (this != &o) { release(); p = o.p; n = o.n; s = o.s; o.p = nullptr; o.n = 0; }
+        if (this != &o) { release(); p = o.p; n = o.n; s = o.s; big = o.big; o.p = nullptr; o.n = 0; o.big = 0; }
         return *this;
     }
     void zero() { if (n) JET_CUDA(cudaMemsetAsync(p, 0, sizeof(T) * (size_t)n, s)); }

@@ -1,5 +1,8 @@
-// level_coop.cuh -- the refinement loop of a level as one cooperative
-// persistent kernel (one 1024-thread CTA per SM).
+// level_coop.cuh -- the refinement loop of a level as one persistent grid
+// kernel, in two launch forms: one thread-block cluster of 8-16 CTAs whose
+// phases meet at the hardware cluster barrier (mid-size levels), or a
+// cooperative launch of one 1024-thread CTA per SM with a software grid
+// barrier.
 //
 // Same phases and results as the single-CTA loop (level_cta.cuh) and the
 // multi-kernel path; phases are separated by a grid barrier instead of kernel
@@ -51,9 +54,23 @@ __device__ __forceinline__ bool grid_sync(GridBar* gb, int* err) {
     return ((volatile int*)&gb->abort)[0] == 0;
 }
 
+// Barrier between phases: a hardware cluster barrier when the whole launch is
+// one thread-block cluster (CL), else the bounded software grid barrier.
+// barrier.cluster with release/acquire orders every memory access of the
+// cluster's threads, global memory included.
+template <bool CL>
+__device__ __forceinline__ bool level_sync(GridBar* gb, int* err) {
+    if constexpr (CL) {
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+        return true;
+    } else {
+        return grid_sync(gb, err);
+    }
+}
+
 // Grid-wide exclusive scan of get(0..n) into out: each block owns a
 // contiguous range; block offsets come from the per-block sums.
-template <class T, class Get>
+template <bool CL, class T, class Get>
 __device__ __forceinline__ bool grid_scan(Get get, int64_t n, T* out, T* block_sums, GridBar* gb, int* err) {
     __shared__ T sw[32];
     __shared__ T s_off;
@@ -64,7 +81,7 @@ __device__ __forceinline__ bool grid_scan(Get get, int64_t n, T* out, T* block_s
     T tot;
     block_exclusive_scan<T>(s, sw, tot);
     if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
-    if (!grid_sync(gb, err)) return false;
+    if (!level_sync<CL>(gb, err)) return false;
     // offset of this block: sum of earlier blocks' sums
     T o = 0;
     for (unsigned b = threadIdx.x; b < blockIdx.x; b += blockDim.x) o += block_sums[b];
@@ -81,13 +98,13 @@ __device__ __forceinline__ bool grid_scan(Get get, int64_t n, T* out, T* block_s
         if (i < hi) out[i] = carry + ex;
         carry += t2;
     }
-    return grid_sync(gb, err);
+    return level_sync<CL>(gb, err);
 }
 
 // One stable LSD pass over 8 bits: keys/values from the functors into
 // (kd, vd).  Blocks own contiguous ranges, processed in order in tiles of
 // blockDim elements, so equal digits keep their input order.
-template <class K, class V, class GetK, class GetV>
+template <bool CL, class K, class V, class GetK, class GetV>
 __device__ __forceinline__ bool grid_radix_pass(GetK getk, GetV getv, int64_t n, int shift, K* kd, V* vd, uint32_t* hist,
                                                 uint32_t (*cnt)[RS_BINS], GridBar* gb, int* err) {
     __shared__ uint32_t base_off[RS_BINS];
@@ -102,7 +119,7 @@ __device__ __forceinline__ bool grid_radix_pass(GetK getk, GetV getv, int64_t n,
     for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&base_off[rs_digit<K>(getk(i), shift)], 1u);
     __syncthreads();
     for (int d = threadIdx.x; d < RS_BINS; d += blockDim.x) hist[(int64_t)d * nb + blockIdx.x] = base_off[d];
-    if (!grid_sync(gb, err)) return false;
+    if (!level_sync<CL>(gb, err)) return false;
     // start of each digit for this block: every smaller digit + this digit in earlier blocks
     {
         const int d = threadIdx.x;  // blockDim >= RS_BINS
@@ -146,7 +163,7 @@ __device__ __forceinline__ bool grid_radix_pass(GetK getk, GetV getv, int64_t n,
         for (int d = threadIdx.x; d < RS_BINS; d += blockDim.x) run[d] += tile_tot[d];
         __syncthreads();
     }
-    return grid_sync(gb, err);
+    return level_sync<CL>(gb, err);
 }
 
 template <class O, class E, class W>
@@ -163,10 +180,10 @@ struct CoopScratch {
 };
 
 // Rebalance tail over the grid (sort_candidates + k_evict_sorted [+ strong]).
-template <bool STRONG, class O, class E, class W>
+template <bool CL, bool STRONG, class O, class E, class W>
 __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>& rb, CoopScratch<O, E, W>& cs, int bits) {
     int* err = &a.dev->err;
-    if (!grid_scan<W>(GetArray<W>{rb.buckets}, (int64_t)rb.t_minibuckets + 1, rb.boff, cs.wsum, cs.bar, err)) return false;
+    if (!grid_scan<CL, W>(GetArray<W>{rb.buckets}, (int64_t)rb.t_minibuckets + 1, rb.boff, cs.wsum, cs.bar, err)) return false;
     const int64_t n = a.g.n;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t(*cnt)[RS_BINS] = (uint32_t(*)[RS_BINS])smem_raw;  // 32 x 256 counters (dynamic shared memory)
@@ -179,31 +196,31 @@ __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>
         O* vd = (p & 1) ? cs.sv1 : cs.sv0;
         bool ok;
         if (p == 0)
-            ok = grid_radix_pass<uint32_t, O>(GetBidKey<O>{rb.bid, rb.none_key}, GetIndex<O>{}, n, 0, kd, vd, cs.hist, cnt, cs.bar, err);
+            ok = grid_radix_pass<CL, uint32_t, O>(GetBidKey<O>{rb.bid, rb.none_key}, GetIndex<O>{}, n, 0, kd, vd, cs.hist, cnt, cs.bar, err);
         else
-            ok = grid_radix_pass<uint32_t, O>(GetArray<uint32_t>{kin}, GetArray<O>{vin}, n, 8 * p, kd, vd, cs.hist, cnt, cs.bar, err);
+            ok = grid_radix_pass<CL, uint32_t, O>(GetArray<uint32_t>{kin}, GetArray<O>{vin}, n, 8 * p, kd, vd, cs.hist, cnt, cs.bar, err);
         if (!ok) return false;
         kin = kd;
         vin = vd;
     }
     rb.skey = kin;
     rb.sval = vin;
-    if (!grid_scan<W>(GetSortedWeight<O, W>{kin, vin, a.g.vw, rb.none_key}, n, cs.wpre, cs.wsum, cs.bar, err)) return false;
+    if (!grid_scan<CL, W>(GetSortedWeight<O, W>{kin, vin, a.g.vw, rb.none_key}, n, cs.wpre, cs.wsum, cs.bar, err)) return false;
     rb.wpre = cs.wpre;
     if (STRONG) {
         for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.k; p += gridDim.x * blockDim.x) rb.evict_adjust[p] = 0;
-        if (!grid_sync(cs.bar, err)) return false;
+        if (!level_sync<CL>(cs.bar, err)) return false;
     }
     if (STRONG) d_evict_sorted<true, O, E, W>(a, rb);
     else d_evict_sorted<false, O, E, W>(a, rb);
-    if (!grid_sync(cs.bar, err)) return false;
+    if (!level_sync<CL>(cs.bar, err)) return false;
     if (STRONG) {
         if (blockIdx.x == 0) d_cookie<O, E, W>(a, rb);
-        if (!grid_sync(cs.bar, err)) return false;
+        if (!level_sync<CL>(cs.bar, err)) return false;
         d_strong_first<O, E, W>(a, rb);
-        if (!grid_sync(cs.bar, err)) return false;
+        if (!level_sync<CL>(cs.bar, err)) return false;
         if (blockIdx.x == 0) d_strong_redraw<O, E, W>(a, rb);
-        if (!grid_sync(cs.bar, err)) return false;
+        if (!level_sync<CL>(cs.bar, err)) return false;
     }
     return true;
 }
@@ -213,14 +230,14 @@ __device__ __forceinline__ void coop_zero(W* p, int64_t m) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) p[i] = 0;
 }
 
-template <class O, class E, class W>
+template <bool CL, class O, class E, class W>
 __global__ void __launch_bounds__(CTA_THREADS, 1)
 k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, W> rbs, Ctl<W>* c, part_t* best_part,
              W* sizes_best, CoopScratch<O, E, W> cs, int bits, int max_iters) {
     int* err = &a.dev->err;
     const O n = a.g.n;
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl_begin_logic(c);
-    if (!grid_sync(cs.bar, err)) return;
+    if (!level_sync<CL>(cs.bar, err)) return;
     int iters = 0;
     while (true) {
         const int more = ((volatile Ctl<W>*)c)->more;
@@ -230,25 +247,25 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             d_lp_select_thread<O, E, W>(a);
             d_lp_select_warp<O, E, W>(a, li.warp_list, li.n_warp);
             d_lp_select_warp<O, E, W>(a, li.hub_list, li.n_hub);
-            if (!grid_sync(cs.bar, err)) return;
+            if (!level_sync<CL>(cs.bar, err)) return;
             switch (li.group) {
                 case 4: d_afterburn<4, O, E, W>(a); break;
                 case 8: d_afterburn<8, O, E, W>(a); break;
                 case 16: d_afterburn<16, O, E, W>(a); break;
                 default: d_afterburn<32, O, E, W>(a); break;
             }
-            if (!grid_sync(cs.bar, err)) return;
+            if (!level_sync<CL>(cs.bar, err)) return;
             d_afterburn_hub<O, E, W>(a);
-            if (!grid_sync(cs.bar, err)) return;
+            if (!level_sync<CL>(cs.bar, err)) return;
         } else {
             RebArgs<O, W>& rb = mode == MODE_WEAK ? rbw : rbs;
             coop_zero<O, E, W>(rb.buckets, (int64_t)rb.t_minibuckets + 1 + rb.width);
-            if (!grid_sync(cs.bar, err)) return;
+            if (!level_sync<CL>(cs.bar, err)) return;
             if (blockIdx.x == 0) {
                 if (mode == MODE_WEAK) d_weak_prep<O, E, W>(a, rb);
                 else d_strong_prep<O, E, W>(a, rb);
             }
-            if (!grid_sync(cs.bar, err)) return;
+            if (!level_sync<CL>(cs.bar, err)) return;
             if (mode == MODE_WEAK) {
                 d_weak_select_thread<O, E, W>(a, rb);
                 d_weak_select_warp<O, E, W>(a, rb, li.warp_list, li.n_warp);
@@ -258,13 +275,13 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
                 d_strong_score_warp<O, E, W>(a, rb, li.warp_list, li.n_warp);
                 d_strong_score_warp<O, E, W>(a, rb, li.hub_list, li.n_hub);
             }
-            if (!grid_sync(cs.bar, err)) return;
-            bool ok = mode == MODE_WEAK ? coop_reb_tail<false, O, E, W>(a, rb, cs, bits) : coop_reb_tail<true, O, E, W>(a, rb, cs, bits);
+            if (!level_sync<CL>(cs.bar, err)) return;
+            bool ok = mode == MODE_WEAK ? coop_reb_tail<CL, false, O, E, W>(a, rb, cs, bits) : coop_reb_tail<CL, true, O, E, W>(a, rb, cs, bits);
             if (!ok) return;
         }
         // perform_moves (src/jet_refiner.hpp:905-955)
         d_apply_moves<O, E, W>(a, 0);
-        if (!grid_sync(cs.bar, err)) return;
+        if (!level_sync<CL>(cs.bar, err)) return;
         switch (li.group) {
             case 4: d_update_small<4, false, O, E, W>(a); break;
             case 8: d_update_small<8, false, O, E, W>(a); break;
@@ -272,7 +289,7 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             default: d_update_small<32, false, O, E, W>(a); break;
         }
         d_update_small_hub<false, O, E, W>(a);
-        if (!grid_sync(cs.bar, err)) return;
+        if (!level_sync<CL>(cs.bar, err)) return;
         switch (li.group) {
             case 4: d_update_small<4, true, O, E, W>(a); d_mark_neighbors<4, O, E, W>(a); break;
             case 8: d_update_small<8, true, O, E, W>(a); d_mark_neighbors<8, O, E, W>(a); break;
@@ -280,7 +297,7 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             default: d_update_small<32, true, O, E, W>(a); d_mark_neighbors<32, O, E, W>(a); break;
         }
         d_update_small_hub<true, O, E, W>(a);
-        if (!grid_sync(cs.bar, err)) return;
+        if (!level_sync<CL>(cs.bar, err)) return;
         if (a.dev->large) {
             // update_large: queue the marked rows (one coalesced pass), then
             // rebuild them one warp per row
@@ -290,12 +307,12 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
                 int64_t s = warp_append(&cs.bar->nmarked, take);
                 if (take) cs.marked[s] = (O)i;
             }
-            if (!grid_sync(cs.bar, err)) return;
+            if (!level_sync<CL>(cs.bar, err)) return;
             d_conn_warp<O, E, W>(a, cs.marked, (O)((volatile GridBar*)cs.bar)->nmarked, 1, nullptr);
-            if (!grid_sync(cs.bar, err)) return;
+            if (!level_sync<CL>(cs.bar, err)) return;
         }
         d_cut_after<O, E, W>(a);
-        if (!grid_sync(cs.bar, err)) return;
+        if (!level_sync<CL>(cs.bar, err)) return;
         if (blockIdx.x == 0) {
             W mx = block_max_sizes<W>(a.sizes, a.k);
             if (threadIdx.x == 0) {
@@ -304,13 +321,13 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
                 if (c->more && ++iters >= max_iters) { c->more = 0; atomicOr(err, ERRF_SPIN); }
             }
         }
-        if (!grid_sync(cs.bar, err)) return;
+        if (!level_sync<CL>(cs.bar, err)) return;
         if (((volatile Ctl<W>*)c)->copy) {
             for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
                 best_part[i] = a.part[i];
             for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.k; p += gridDim.x * blockDim.x) sizes_best[p] = a.sizes[p];
         }
-        if (!grid_sync(cs.bar, err)) return;
+        if (!level_sync<CL>(cs.bar, err)) return;
     }
 }
 

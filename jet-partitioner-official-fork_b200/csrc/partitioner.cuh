@@ -312,33 +312,45 @@ struct Engine {
         return match_map(L, alg == 0, seed, level, vcmap, hn_out);
     }
 
-    // Puts the hub rows of C (coarse vertices list[0..nhub)) in neighbour order:
-    // one stable radix sort of (row rank, neighbour id) keys over their entries.
-    void sort_hub_rows(const O* list, int64_t nhub, O nc, Level<O, E, W>& C) {
-        DBuf<E> hoff(nhub + 1, s);
-        E* tot = dslot<E>(45);
-        exclusive_scan<E, GetHubRowSize<O, E>>(GetHubRowSize<O, E>{list, C.own_row.p}, nhub, hoff.p, tot, scan, s);
-        JET_CUDA(cudaMemcpyAsync(&hscal[5], tot, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    // Hub rows of a level with many coarse ids (see k_hub_keys): keys, one
+    // radix sort, reduce-by-key into the rows' scratch regions.
+    void contract_hubs_sorted(GView<O, E, W> g, const O* map, const O* lh, const O* nh, const O* moff, const O* members,
+                              const E* hrow, O nc, O* skey, W* sval, O* ucnt) {
+        JET_CUDA(cudaMemcpyAsync(&hscal[6], nh, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
         sync();
-        int64_t total = (int64_t)*(E*)&hscal[5];
-        if (total <= 1) return;
-        int nb = bits_for((uint64_t)nc);
-        int bits = nb + bits_for((uint64_t)nhub);
+        int64_t nhub = (int64_t)*(O*)&hscal[6];
+        if (nhub <= 0) return;
+        DBuf<E> hoff(nhub + 1, s);
+        E* tot = dslot<E>(46);
+        exclusive_scan<E, GetHubDu<O, E>>(GetHubDu<O, E>{lh, hrow}, nhub, hoff.p, tot, scan, s);
+        JET_CUDA(cudaMemcpyAsync(&hscal[7], tot, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        sync();
+        int64_t total = (int64_t)*(E*)&hscal[7];
+        if (total <= 0) return;
+        const int nb = bits_for((uint64_t)nc);
+        const uint64_t sentinel = (uint64_t)nhub << nb;
+        const int bits = bits_for(sentinel);
         if (bits > 64) throw JetError{JET_ERR_INVALID, "hub row sort key exceeds 64 bits"};
-        DBuf<uint64_t> k0(total, s), k1(total, s);
-        DBuf<int64_t> v0(total, s), v1(total, s);
-        DBuf<W> tval(total, s);
-        int which = radix_sort_pairs<uint64_t, int64_t>(GetHubKey<O, E>{list, C.own_row.p, hoff.p, nhub, C.own_adj.p, nb},
-                                                        GetIndex<int64_t>{}, total, bits, k0.p, v0.p, k1.p, v1.p, rsort, scan, s);
+        DBuf<uint64_t> kin(total, s), k0(total, s), k1(total, s);
+        DBuf<W> vin(total, s), v0(total, s), v1(total, s);
+        k_hub_keys<O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(g, map, lh, nh, moff, members, hoff.p, nb, sentinel, kin.p,
+                                                                   vin.p); count_launch();
+        JET_LAUNCH_CHECK();
+        int which = radix_sort_pairs<uint64_t, W>(GetArray<uint64_t>{kin.p}, GetArray<W>{vin.p}, total, bits, k0.p, v0.p, k1.p,
+                                                  v1.p, rsort, scan, s);
         const uint64_t* sk = which == 0 ? k0.p : k1.p;
-        const int64_t* sq = which == 0 ? v0.p : v1.p;
+        const W* sv = which == 0 ? v0.p : v1.p;
+        DBuf<int64_t> seg(total, s), row_first(nhub, s);
+        exclusive_scan<int64_t, GetKeyHead<uint64_t, int64_t>>(GetKeyHead<uint64_t, int64_t>{sk, sentinel}, total, seg.p, nullptr,
+                                                               scan, s);
         unsigned grid = grid_persistent(total, 16);
-        k_hub_gather<O, E, W><<<grid, BLOCK, 0, s>>>(list, C.own_row.p, hoff.p, nhub, total, sq, C.own_val.p, tval.p); count_launch();
-        k_hub_place<O, E, W><<<grid, BLOCK, 0, s>>>(list, C.own_row.p, hoff.p, total, sk, tval.p, nb, C.own_adj.p, C.own_val.p); count_launch();
+        k_hub_row_first<<<grid, BLOCK, 0, s>>>(sk, total, nb, sentinel, seg.p, row_first.p); count_launch();
+        k_hub_reduce<O, E, W><<<grid, BLOCK, 0, s>>>(sk, sv, total, nb, sentinel, seg.p, row_first.p, lh, hrow, skey, sval, ucnt); count_launch();
         JET_LAUNCH_CHECK();
     }
 
     // ------------------------------------------------------------ contraction
+    static constexpr int DENSE_PASSES = 8;
     // build_coarse_graph, src/contract.hpp:347-446.
     void contract(const Level<O, E, W>& L, const O* map, O nc, Level<O, E, W>& C, DBuf<O>* skey_buf, DBuf<W>* sval_buf) {
         auto g = L.view();
@@ -365,6 +377,14 @@ struct Engine {
         O* n2 = dslot<O>(41);
         O* nh = dslot<O>(42);
         int* err = dslot<int>(43);
+        // hub rows: a dense shared-memory accumulator when the coarse id range
+        // takes at most DENSE_PASSES chunks, else (row, neighbour) keys + radix sort
+        int dense_chunk = (max_dynamic_smem((const void*)k_contract_dense<O, E, W>) - 1024) / (int)sizeof(W);
+        dense_chunk &= ~1023;
+        const bool dense = dense_chunk > 0 && (int64_t)nc <= (int64_t)DENSE_PASSES * dense_chunk;
+        if (dense)
+            JET_CUDA(cudaFuncSetAttribute(k_contract_dense<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          max_dynamic_smem((const void*)k_contract_dense<O, E, W>)));
         JET_CUDA(cudaMemsetAsync(n1, 0, 4 * sizeof(int64_t), s));
         k_contract_bin<O, E><<<grid_persistent(nc, 8), BLOCK, 0, s>>>(nc, hrow.p, l1.p, n1, l2.p, n2, lh.p, nh); count_launch();
         JET_LAUNCH_CHECK();
@@ -380,8 +400,13 @@ struct Engine {
             k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W><<<device_info().sms * 2, CT_S2_THREADS, sm2, s>>>(
                 g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p); count_launch();
             JET_LAUNCH_CHECK();
-            k_contract_hub<O, E, W><<<device_info().sms, 1024, 0, s>>>(g, map, lh.p, nh, moff.p, members.p, hrow.p, skey, sval, ucnt.p, err); count_launch();
-            JET_LAUNCH_CHECK();
+            if (dense) {
+                k_contract_dense<O, E, W><<<device_info().sms, 1024, (size_t)dense_chunk * sizeof(W), s>>>(
+                    g, map, lh.p, nh, moff.p, members.p, hrow.p, nc, dense_chunk, skey, sval, ucnt.p); count_launch();
+                JET_LAUNCH_CHECK();
+            } else {
+                contract_hubs_sorted(g, map, lh.p, nh, moff.p, members.p, hrow.p, nc, skey, sval, ucnt.p);
+            }
         }
         // coarse row offsets and nnz
         C.own_row.alloc(nc + 1, s);
@@ -395,13 +420,10 @@ struct Engine {
         C.m = mc;
         C.own_adj.alloc(mc > 0 ? mc : 1, s);
         C.own_val.alloc(mc > 0 ? mc : 1, s);
+        // every row's unique entries are packed at its scratch offset, in neighbour order
         k_contract_copy<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(nc, hrow.p, skey, sval, C.own_row.p,
                                                                                         C.own_adj.p, C.own_val.p); count_launch();
         JET_LAUNCH_CHECK();
-        k_contract_copy_hub<O, E, W><<<device_info().sms, 1024, 0, s>>>(lh.p, nh, hrow.p, skey, sval, C.own_row.p, C.own_adj.p, C.own_val.p); count_launch();
-        JET_LAUNCH_CHECK();
-        int64_t nhub = (int64_t)*(O*)&hscal[2];
-        if (nhub > 0) sort_hub_rows(lh.p, nhub, nc, C);
         C.row = C.own_row.p;
         C.adj = C.own_adj.p;
         C.val = C.own_val.p;

@@ -3,6 +3,7 @@
 // profiling and the tier-generic C entry points.
 #include "api_impl.cuh"
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <mutex>
 #include <string>
@@ -62,6 +63,73 @@ cudaMemPool_t pool_for_current_device() {
     return pools[dev];
 }
 
+namespace {
+struct BigBlock {
+    void* p;
+    size_t bytes;
+    int dev;
+    cudaEvent_t ev;  // recorded on the freeing stream
+};
+std::mutex g_big_mu;
+std::vector<BigBlock> g_big_free;
+size_t g_big_cached = 0;
+}  // namespace
+
+void* big_alloc(size_t bytes, cudaStream_t s, size_t* got) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lk(g_big_mu);
+        int best = -1;
+        for (size_t i = 0; i < g_big_free.size(); i++) {
+            const BigBlock& b = g_big_free[i];
+            if (b.dev == dev && b.bytes >= bytes && b.bytes <= 2 * bytes && (best < 0 || b.bytes < g_big_free[best].bytes))
+                best = (int)i;
+        }
+        if (best >= 0) {
+            BigBlock b = g_big_free[best];
+            g_big_free.erase(g_big_free.begin() + best);
+            g_big_cached -= b.bytes;
+            JET_CUDA(cudaStreamWaitEvent(s, b.ev, 0));
+            cudaEventDestroy(b.ev);
+            *got = b.bytes;
+            return b.p;
+        }
+    }
+    void* p = nullptr;
+    JET_CUDA(cudaMallocFromPoolAsync(&p, bytes, pool_for_current_device(), s));
+    *got = bytes;
+    return p;
+}
+
+void big_free(void* p, size_t bytes, cudaStream_t s) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaEvent_t ev;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess || cudaEventRecord(ev, s) != cudaSuccess) {
+        cudaFreeAsync(p, s);
+        return;
+    }
+    std::lock_guard<std::mutex> lk(g_big_mu);
+    g_big_free.push_back({p, bytes, dev, ev});
+    g_big_cached += bytes;
+    // keep at most a quarter of this device's memory cached; oldest blocks go first
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    size_t mine = 0;
+    for (const BigBlock& b : g_big_free) if (b.dev == dev) mine += b.bytes;
+    for (size_t i = 0; i < g_big_free.size() && mine > total_b / 4;) {
+        BigBlock b = g_big_free[i];
+        if (b.dev != dev) { i++; continue; }
+        g_big_free.erase(g_big_free.begin() + i);
+        g_big_cached -= b.bytes;
+        mine -= b.bytes;
+        cudaStreamWaitEvent(s, b.ev, 0);
+        cudaFreeAsync(b.p, s);
+        cudaEventDestroy(b.ev);
+    }
+}
+
 cudaStream_t default_stream() {
     static cudaStream_t streams[64] = {};
     int dev = 0;
@@ -77,6 +145,9 @@ int64_t launch_counter() { return g_launches.load(); }
 static std::atomic<int> g_drivers{JET_DRIVER_ALL};
 static thread_local int t_driver_mask = JET_DRIVER_ALL;
 int refine_drivers() { return g_drivers.load() & t_driver_mask; }
+double host_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 bool debug_timing() {
     static const bool on = getenv("JET_DEBUG_TIMING") != nullptr;
     return on;
@@ -412,8 +483,9 @@ int jet_set_refine_drivers(int mask) { return g_drivers.exchange(mask & JET_DRIV
 // Batch and server workers run many partitions side by side.  A cooperative
 // level kernel needs every SM at once and would stall the other streams, and
 // building a level graph costs more host time than its launches save when
-// the GPU is shared, so their threads keep only the one-CTA level loop (the
-// host loop takes the larger levels).  They also wait on streams without
+// the GPU is shared, and a 16-CTA cluster must wait for 16 free SMs, so their
+// threads keep only the one-CTA level loop (the host loop takes the larger
+// levels).  They also wait on streams without
 // spinning and send Metis calls to helper processes.
 void jet_thread_batch_mode(int on) {
     t_driver_mask = on ? JET_DRIVER_CTA : JET_DRIVER_ALL;

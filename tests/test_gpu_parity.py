@@ -291,15 +291,16 @@ def test_edge_cases(jet, graphs, orc):
     assert orc.pstat(orc.G.from_csr(small), p, 3)[0] == cut
 
 
-@pytest.mark.parametrize("drivers", ["all", "no_cta", "graph", "host"])
+@pytest.mark.parametrize("drivers", ["all", "cluster", "coop", "graph", "host"])
 @pytest.mark.parametrize("tier,kind,k", [("i32", "grid2d", 16), ("big", "rgg", 64), ("biggest", "grid2d", 300),
                                          ("i32", "rgg", 600)])
 def test_level_drivers_bit_exact(jet, graphs, orc, drivers, tier, kind, k):
-    """Every level-loop driver (one CTA, cooperative grid kernel, CUDA graph
-    with conditional nodes, host loop) returns the oracle's partition on
-    graphs whose finer levels exceed the one-CTA bound."""
-    mask = {"all": jet.DRIVER_ALL, "no_cta": jet.DRIVER_COOP | jet.DRIVER_GRAPH, "graph": jet.DRIVER_GRAPH,
-            "host": 0}[drivers]
+    """Every level-loop driver (one CTA, one thread-block cluster, cooperative
+    grid kernel, CUDA graph with conditional nodes, host loop) returns the
+    oracle's partition on graphs whose finer levels exceed the one-CTA
+    bound."""
+    mask = {"all": jet.DRIVER_ALL, "cluster": jet.DRIVER_CLUSTER, "coop": jet.DRIVER_COOP | jet.DRIVER_GRAPH,
+            "graph": jet.DRIVER_GRAPH, "host": 0}[drivers]
     g = graphs.grid2d(170, 150, weighted=True, seed=7) if kind == "grid2d" else graphs.rgg(30000, 9.0, seed=5)
     g = g.as_tier(tier)
     og = orc.G.from_csr(g)
@@ -334,3 +335,25 @@ def test_full_size_partition_bit_exact(jet, graphs, orc, wl):
         part, cut, _ = fn(cfg, gd, seed=1)
         assert cut == wcut
         assert np.array_equal(host(part), want)
+
+
+@pytest.mark.parametrize("tier", ["i32", "big"])
+@pytest.mark.parametrize("n", [20001, 1200001])
+def test_contract_hub_rows_both_paths(jet, graphs, orc, tier, n):
+    """A ring plus a hub of degree 6000: with few coarse vertices the hub row
+    goes through the dense shared-memory accumulator, with many (> 8 chunks
+    of ids) through the global hash table and the hub-row sort.  Both give
+    the oracle's rows exactly."""
+    hub_deg = 6000
+    u = torch.cat([torch.zeros(hub_deg, dtype=torch.long), torch.arange(1, n - 1)])
+    v = torch.cat([torch.arange(1, hub_deg + 1) * ((n - 1) // hub_deg), torch.arange(2, n)])
+    w = torch.randint(1, 9, (u.numel(),), generator=torch.Generator().manual_seed(n))
+    g = graphs.from_undirected(n, u, v, w).as_tier(tier)
+    og = orc.G.from_csr(g)
+    m, nc, _ = orc.coarsen(og, 1, level=2, seed=3, uniform=False)
+    want = orc.contract(og, m, nc)
+    got = jet.contract(g.to("cuda"), torch.from_numpy(m).cuda(), nc)
+    assert np.array_equal(host(got.row), want.row)
+    assert np.array_equal(host(got.adj), want.adj)
+    assert np.array_equal(host(got.val), want.val)
+    assert np.array_equal(host(got.vw), want.vw)
