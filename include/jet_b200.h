@@ -98,6 +98,21 @@ int jet_partition_biggest(const jet_config_c* config, int64_t n, const int64_t* 
                           const int64_t* values, const int64_t* vweights, int uniform_ew, int mem, uint64_t seed,
                           void* stream, int32_t* part_out, int64_t* edge_cut, jet_stats_c* stats);
 
+/* ---------------------------------------------------------------- hierarchy dump and import
+ * With config.dump_coarse set, a partition call writes, as the reference
+ * does (src/uncoarsen.hpp:93-111, src/binary_dump.hpp:61-97), the files
+ * "coarse_graphs.out" (the levels from the finest down to the first level
+ * whose partition is balanced before refinement, in the reference's binary
+ * layout with this tier's types) and "coarse_part.out" (that level's
+ * partition) in the working directory.
+ * jet_refine_hierarchy replaces app/import_coarse.cpp:49-132: it reads such
+ * files (NULL paths = those names), refines from their coarsest level down
+ * and writes the finest partition to part_out (host memory, part_capacity
+ * entries at least; *n_out receives the finest vertex count).  Imported
+ * levels are treated as non-uniform, as in the reference. */
+int jet_refine_hierarchy(int tier, const jet_config_c* config, const char* graphs_path, const char* part_path, int32_t* part_out,
+                         int64_t part_capacity, int64_t* n_out, int64_t* edge_cut, jet_stats_c* stats, void* stream);
+
 /* ---------------------------------------------------------------- batched
  * Many graphs of one tier in one call (no counterpart in the reference,
  * which partitions one graph per call).  Each graph is an independent

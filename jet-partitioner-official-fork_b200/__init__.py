@@ -20,6 +20,7 @@ from __future__ import annotations
 import ctypes
 import os
 from dataclasses import dataclass, field
+import numpy as np
 from typing import List, Optional
 
 import torch
@@ -55,7 +56,7 @@ EXPORTED_SYMBOLS = [
     "jet_conn_build", "jet_refine_iters", "jet_refine_level", "jet_pstat", "jet_project", "jet_version",
     "jet_last_error", "jet_device_ok", "jet_prof_enable", "jet_prof_read", "jet_launch_count", "jet_pstat_noalloc",
     "jet_set_refine_drivers", "jet_partition_batch", "jet_server_create", "jet_server_submit", "jet_server_wait",
-    "jet_server_footprint", "jet_server_stats_get", "jet_server_destroy",
+    "jet_server_footprint", "jet_server_stats_get", "jet_server_destroy", "jet_refine_hierarchy",
 ]
 
 # level-loop drivers (jet_set_refine_drivers)
@@ -438,6 +439,31 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def refine_hierarchy(config: config_t, tier: str = "i32", graphs_path: Optional[str] = None,
+                     part_path: Optional[str] = None, capacity: Optional[int] = None):
+    """Refines a dumped hierarchy (jet_refine_hierarchy, the import_coarse
+    app of the reference): returns (part, edge_cut, experiment)."""
+    _require_cuda()
+    lib = load()
+    if capacity is None:
+        with open(graphs_path or "coarse_graphs.out", "rb") as f:
+            f.read(4)
+            capacity = int(np.frombuffer(f.read(8 if tier == "biggest" else 4), dtype=np.int64 if tier == "biggest" else np.int32)[0])
+    part = np.empty(max(capacity, 1), dtype=np.int32)
+    n = ctypes.c_int64(0)
+    cut = ctypes.c_int64(0)
+    st = jet_stats_c()
+    cfg = config.to_c()
+    gp = graphs_path.encode() if graphs_path else None
+    pp = part_path.encode() if part_path else None
+    _check(lib.jet_refine_hierarchy(TIER_ID[tier], ctypes.byref(cfg), ctypes.c_char_p(gp), ctypes.c_char_p(pp),
+                                    part.ctypes.data_as(ctypes.c_void_p), ctypes.c_int64(capacity), ctypes.byref(n),
+                                    ctypes.byref(cut), ctypes.byref(st), _stream_ptr()))
+    exp = experiment_data()
+    exp.fill(st)
+    return torch.from_numpy(part[:n.value].copy()), int(cut.value), exp
 
 
 def assign_lpt(costs, world_size: int):

@@ -123,7 +123,7 @@ int partition_impl(const jet_config_c* cfg, O n, const E* row, const O* adj, con
         part_t* pout = part_out;
         if (mem == JET_MEM_HOST) { part_dev.alloc(n, s); pout = part_dev.p; }
         Cfg c{cfg->coarsening_alg, cfg->num_parts, cfg->max_imb_ratio, cfg->refine_tolerance, cfg->ultra_settings != 0,
-              cfg->verbose != 0};
+              cfg->verbose != 0, cfg->dump_coarse != 0};
         if (c.k == 1) {
             // a single part: everything in part 0, nothing cut
             JET_CUDA(cudaMemsetAsync(pout, 0, sizeof(part_t) * n, s));
@@ -354,6 +354,94 @@ struct Tier {
             return JET_OK;
         });
     }
+
+    // app/import_coarse.cpp:49-132: load a dumped hierarchy (reference
+    // layout, this tier's types) and its coarsest partition, then uncoarsen.
+    static int refine_hierarchy(const jet_config_c* cfg, const char* graphs_path, const char* part_path, int32_t* part_out,
+                                int64_t part_capacity, int64_t* n_out, int64_t* cut_out, jet_stats_c* st, void* stream) {
+        return guarded([&]() -> int {
+            if (!cfg || !part_out || !cut_out) throw JetError{JET_ERR_INVALID, "null argument"};
+            if (st) std::memset(st, 0, sizeof(*st));
+            const char* gp = graphs_path ? graphs_path : "coarse_graphs.out";
+            const char* pp = part_path ? part_path : "coarse_part.out";
+            Engine<O, E, W> eng(pick_stream(stream));
+            cudaStream_t s = eng.s;
+            auto t_start = clk::now();
+            double meas[JET_NUM_MEASUREMENTS] = {0};
+            FILE* f = fopen(gp, "rb");
+            if (!f) throw JetError{JET_ERR_INVALID, "cannot open the hierarchy file"};
+            std::vector<std::unique_ptr<Level<O, E, W>>> levels;
+            int size = 0;
+            bool ok = fread(&size, sizeof(int), 1, f) == 1 && size > 0 && size <= 1000;
+            O prev_n = 0;
+            for (int l = 0; ok && l < size; l++) {
+                O n = 0;
+                E m = 0;
+                ok = fread(&n, sizeof(O), 1, f) == 1 && fread(&m, sizeof(E), 1, f) == 1 && n >= 0 && m >= 0;
+                if (!ok) break;
+                std::vector<E> row(n + 1);
+                std::vector<O> adj(m), map(l > 0 ? prev_n : 0);
+                std::vector<W> val(m), vw(n);
+                ok = fread(row.data(), sizeof(E), n + 1, f) == (size_t)(n + 1) && fread(adj.data(), sizeof(O), m, f) == (size_t)m &&
+                     fread(val.data(), sizeof(W), m, f) == (size_t)m && fread(vw.data(), sizeof(W), n, f) == (size_t)n &&
+                     fread(map.data(), sizeof(O), map.size(), f) == map.size();
+                if (!ok) break;
+                std::unique_ptr<Level<O, E, W>> L(new Level<O, E, W>());
+                L->n = n;
+                L->m = m;
+                L->own_row.alloc(n + 1, s);
+                L->own_adj.alloc(m > 0 ? m : 1, s);
+                L->own_val.alloc(m > 0 ? m : 1, s);
+                L->own_vw.alloc(n > 0 ? n : 1, s);
+                JET_CUDA(cudaMemcpyAsync(L->own_row.p, row.data(), sizeof(E) * (n + 1), cudaMemcpyHostToDevice, s));
+                if (m) {
+                    JET_CUDA(cudaMemcpyAsync(L->own_adj.p, adj.data(), sizeof(O) * m, cudaMemcpyHostToDevice, s));
+                    JET_CUDA(cudaMemcpyAsync(L->own_val.p, val.data(), sizeof(W) * m, cudaMemcpyHostToDevice, s));
+                }
+                if (n) JET_CUDA(cudaMemcpyAsync(L->own_vw.p, vw.data(), sizeof(W) * n, cudaMemcpyHostToDevice, s));
+                if (l > 0) {
+                    L->map.alloc(prev_n > 0 ? prev_n : 1, s);
+                    if (prev_n) JET_CUDA(cudaMemcpyAsync(L->map.p, map.data(), sizeof(O) * prev_n, cudaMemcpyHostToDevice, s));
+                }
+                stream_wait(s);  // host vectors go out of scope
+                L->row = L->own_row.p;
+                L->adj = L->own_adj.p;
+                L->val = L->own_val.p;
+                L->vw = L->own_vw.p;
+                L->uniform = false;  // imported levels carry no uniform flag (reference default)
+                eng.prepare_level(*L);
+                levels.push_back(std::move(L));
+                prev_n = n;
+            }
+            fclose(f);
+            if (!ok) throw JetError{JET_ERR_INVALID, "malformed hierarchy file"};
+            validate<O, E, W>(eng, levels[0]->n, levels[0]->m, levels[0]->row, levels[0]->adj, levels[0]->val, levels[0]->vw);
+            O n0 = levels[0]->n, nc = levels.back()->n;
+            if (n_out) *n_out = (int64_t)n0;
+            if ((int64_t)n0 > part_capacity) throw JetError{JET_ERR_INVALID, "part_out too small for the finest level"};
+            DBuf<part_t> pa(n0 > 0 ? n0 : 1, s), pb(n0 > 0 ? n0 : 1, s), pout(n0 > 0 ? n0 : 1, s);
+            {
+                std::vector<part_t> cp(nc);
+                FILE* pf = fopen(pp, "rb");
+                bool pok = pf && fread(cp.data(), sizeof(part_t), nc, pf) == (size_t)nc;
+                if (pf) fclose(pf);
+                if (!pok) throw JetError{JET_ERR_INVALID, "cannot read the coarse partition file"};
+                for (part_t p : cp)
+                    if (p < 0 || p >= cfg->num_parts) throw JetError{JET_ERR_INVALID, "part id out of range in the coarse partition"};
+                if (nc) JET_CUDA(cudaMemcpyAsync(pa.p, cp.data(), sizeof(part_t) * nc, cudaMemcpyHostToDevice, s));
+                stream_wait(s);
+            }
+            Cfg c{cfg->coarsening_alg, cfg->num_parts, cfg->max_imb_ratio, cfg->refine_tolerance, cfg->ultra_settings != 0,
+                  cfg->verbose != 0, false};
+            double t_load = since(t_start);
+            W cut = uncoarsen_levels<O, E, W>(eng, c, levels, pa, pb, pout.p, st, meas, t_start, 0.0, (int64_t)nc);
+            if (st) st->measurements[M_INITPARTITION] = t_load;
+            if (n0) JET_CUDA(cudaMemcpyAsync(part_out, pout.p, sizeof(part_t) * n0, cudaMemcpyDeviceToHost, s));
+            stream_wait(s);
+            *cut_out = (int64_t)cut;
+            return JET_OK;
+        });
+    }
 };
 
 // Per-tier function table used by the tier-generic entry points.
@@ -370,12 +458,15 @@ struct TierOps {
                         int64_t*, int32_t*, void*);
     int (*pstat)(int64_t, int64_t, const void*, const void*, const void*, const void*, const int32_t*, int32_t, int64_t*, void*);
     int (*project)(int64_t, const void*, const int32_t*, int32_t*, void*);
+    int (*refine_hierarchy)(const jet_config_c*, const char*, const char*, int32_t*, int64_t, int64_t*, int64_t*, jet_stats_c*,
+                            void*);
 };
 
 template <class O, class E, class W>
 TierOps make_ops() {
     using T = Tier<O, E, W>;
-    return TierOps{&T::coarsen_map, &T::contract, &T::conn_build, &T::refine_iters, &T::refine_level, &T::pstat, &T::project};
+    return TierOps{&T::coarsen_map, &T::contract, &T::conn_build, &T::refine_iters, &T::refine_level, &T::pstat, &T::project,
+                   &T::refine_hierarchy};
 }
 
 TierOps ops_i32();

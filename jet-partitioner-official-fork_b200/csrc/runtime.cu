@@ -470,6 +470,13 @@ int jet_pstat(int tier, int64_t n, int64_t nnz, const void* row_map, const void*
     return o->pstat(n, nnz, row_map, entries, values, vweights, part, k, out, stream);
 }
 
+int jet_refine_hierarchy(int tier, const jet_config_c* config, const char* graphs_path, const char* part_path, int32_t* part_out,
+                         int64_t part_capacity, int64_t* n_out, int64_t* edge_cut, jet_stats_c* stats, void* stream) {
+    TierOps* o = ops_for(tier);
+    if (!o) return JET_ERR_INVALID;
+    return o->refine_hierarchy(config, graphs_path, part_path, part_out, part_capacity, n_out, edge_cut, stats, stream);
+}
+
 int jet_project(int tier, int64_t n_fine, const void* map, const int32_t* coarse, int32_t* fine, void* stream) {
     TierOps* o = ops_for(tier);
     if (!o) return JET_ERR_INVALID;

@@ -807,7 +807,126 @@ struct Cfg {
     double tol;
     bool ultra;
     bool verbose;
+    bool dump = false;  // config_t::dump_coarse
 };
+
+// Writes the hierarchy levels[0..last] in the reference's binary layout
+// (src/binary_dump.hpp:61-90): int32 level count, then per level N, M,
+// row_map[N+1], entries[M], values[M], vertex weights[N] (tier types) and,
+// from the second level on, the map from the previous level.
+template <class O, class E, class W>
+void dump_hierarchy(const std::vector<std::unique_ptr<Level<O, E, W>>>& levels, int last, const char* path, cudaStream_t s) {
+    FILE* f = fopen(path, "wb");
+    if (!f) throw JetError{JET_ERR_INVALID, "cannot open the hierarchy dump file"};
+    int size = last + 1;
+    bool ok = fwrite(&size, sizeof(int), 1, f) == 1;
+    for (int l = 0; ok && l <= last; l++) {
+        const Level<O, E, W>& L = *levels[l];
+        O n = L.n;
+        E m = L.m;
+        std::vector<E> row(n + 1);
+        std::vector<O> adj(m), map(l > 0 ? levels[l - 1]->n : 0);
+        std::vector<W> val(m), vw(n);
+        JET_CUDA(cudaMemcpyAsync(row.data(), L.row, sizeof(E) * (n + 1), cudaMemcpyDeviceToHost, s));
+        if (m) {
+            JET_CUDA(cudaMemcpyAsync(adj.data(), L.adj, sizeof(O) * m, cudaMemcpyDeviceToHost, s));
+            JET_CUDA(cudaMemcpyAsync(val.data(), L.val, sizeof(W) * m, cudaMemcpyDeviceToHost, s));
+        }
+        if (n) JET_CUDA(cudaMemcpyAsync(vw.data(), L.vw, sizeof(W) * n, cudaMemcpyDeviceToHost, s));
+        if (!map.empty()) JET_CUDA(cudaMemcpyAsync(map.data(), L.map.p, sizeof(O) * map.size(), cudaMemcpyDeviceToHost, s));
+        stream_wait(s);
+        ok = fwrite(&n, sizeof(O), 1, f) == 1 && fwrite(&m, sizeof(E), 1, f) == 1 &&
+             fwrite(row.data(), sizeof(E), n + 1, f) == (size_t)(n + 1) && fwrite(adj.data(), sizeof(O), m, f) == (size_t)m &&
+             fwrite(val.data(), sizeof(W), m, f) == (size_t)m && fwrite(vw.data(), sizeof(W), n, f) == (size_t)n &&
+             fwrite(map.data(), sizeof(O), map.size(), f) == map.size();
+    }
+    if (fclose(f) != 0) ok = false;
+    if (!ok) throw JetError{JET_ERR_INVALID, "writing the hierarchy dump failed"};
+}
+
+// The partition of one level as part_t values (src/binary_dump.hpp:91-97).
+inline void dump_part(const part_t* part_dev, int64_t n, const char* path, cudaStream_t s) {
+    std::vector<part_t> h(n);
+    if (n) JET_CUDA(cudaMemcpyAsync(h.data(), part_dev, sizeof(part_t) * n, cudaMemcpyDeviceToHost, s));
+    stream_wait(s);
+    FILE* f = fopen(path, "wb");
+    bool ok = f && fwrite(h.data(), sizeof(part_t), n, f) == (size_t)n;
+    if (f && fclose(f) != 0) ok = false;
+    if (!ok) throw JetError{JET_ERR_INVALID, "writing the coarse partition dump failed"};
+}
+
+// multilevel_jet + uncoarsen (src/uncoarsen.hpp:88-158): refine from the
+// coarsest level down, projecting between levels.  `pa` holds the coarsest
+// partition; `pb` is a second buffer of the finest size.  With cfg.dump the
+// hierarchy and partition are written, as the reference does, at the first
+// level (from the coarsest) whose partition is balanced before refinement.
+template <class O, class E, class W>
+W uncoarsen_levels(Engine<O, E, W>& eng, const Cfg& cfg, std::vector<std::unique_ptr<Level<O, E, W>>>& levels, DBuf<part_t>& pa,
+                   DBuf<part_t>& pb, part_t* part_out, jet_stats_c* st, double* meas, clk::time_point t_start,
+                   double t_coarsen, int64_t coarsest_n) {
+    cudaStream_t s = eng.s;
+    part_t k = cfg.k;
+    Level<O, E, W>& L0 = *levels[0];
+    auto tr = clk::now();
+    Refiner<O, E, W> ref(eng, L0.n, (int64_t)L0.m, k);
+    ref.verbose = cfg.verbose;
+    part_t* cur_part = pa.p;
+    part_t* other = pb.p;
+    int nl = (int)levels.size();
+    if (st) st->num_levels = nl;
+    bool dumped = !cfg.dump;
+    for (int l = nl - 1; l >= 0; l--) {
+        if (!dumped) {
+            // src/uncoarsen.hpp:96-111 (imbalance as get_max_imb, :69-80)
+            Level<O, E, W>& L = *levels[l];
+            ref.part_sizes(L, cur_part, ref.sizes_curr.p);
+            std::vector<W> hs(k);
+            JET_CUDA(cudaMemcpyAsync(hs.data(), ref.sizes_curr.p, sizeof(W) * k, cudaMemcpyDeviceToHost, s));
+            eng.sync();
+            W mx = 0, tot = 0;
+            for (W x : hs) { if (x > mx) mx = x; tot += x; }
+            O opt = (O)(((O)tot + k - 1) / k);
+            if ((double)mx / (double)opt <= cfg.imb) {
+                dump_part(cur_part, (int64_t)L.n, "coarse_part.out", s);
+                dump_hierarchy<O, E, W>(levels, l, "coarse_graphs.out", s);
+                dumped = true;
+            }
+        }
+        jet_level_stats_c cl = ref.refine(*levels[l], cur_part, cfg.imb, cfg.tol, cfg.ultra);
+        int idx = nl - 1 - l;
+        if (st && idx < JET_MAX_LEVELS) st->levels[idx] = cl;
+        if (l > 0) {
+            Level<O, E, W>& fine = *levels[l - 1];
+            k_project<O><<<grid_persistent(fine.n, 16), BLOCK, 0, s>>>(fine.n, levels[l]->map.p, cur_part, other); count_launch();
+            JET_LAUNCH_CHECK();
+            std::swap(cur_part, other);
+            if (l - 1 > 0) { levels[l].reset(); }
+        }
+    }
+    eng.sync();
+    meas[M_REFINE] += since(tr);
+    JET_CUDA(cudaMemcpyAsync(part_out, cur_part, sizeof(part_t) * L0.n, cudaMemcpyDeviceToDevice, s));
+    W cut_half = ref.best.cut / 2;
+    if (st) {
+        std::vector<W> hs(k);
+        JET_CUDA(cudaMemcpyAsync(hs.data(), ref.sizes_best.p, sizeof(W) * k, cudaMemcpyDeviceToHost, s));
+        eng.sync();
+        W largest = 0, smallest = ref.best.total_size;
+        for (W x : hs) { if (x > largest) largest = x; if (x < smallest) smallest = x; }
+        double opt = (double)(O)(((O)ref.best.total_size + k - 1) / k);
+        st->edge_cut = (int64_t)cut_half;
+        st->imb_ratio = (double)largest / opt;
+        st->largest_part = (int64_t)largest;
+        st->smallest_part = (int64_t)smallest;
+        st->coarsest_vertices = coarsest_n;
+        st->refine_iterations = ref.total_iters;
+        meas[M_COARSEN] = t_coarsen;
+        meas[M_TOTAL] = since(t_start);
+        for (int i = 0; i < JET_NUM_MEASUREMENTS; i++) st->measurements[i] = meas[i];
+    }
+    eng.sync();
+    return cut_half;
+}
 
 template <class O, class E, class W>
 W run_partition(Engine<O, E, W>& eng, const Cfg& cfg, const GraphIn<O, E, W>& in, uint64_t seed, part_t* part_out,
@@ -870,49 +989,7 @@ W run_partition(Engine<O, E, W>& eng, const Cfg& cfg, const GraphIn<O, E, W>& in
     DBuf<part_t> pa(L0.n > 0 ? L0.n : 1, s), pb(L0.n > 0 ? L0.n : 1, s);
     metis_coarsest(coarsest, k, cfg.imb, pa.p, s);
     meas[M_INITPARTITION] += since(ti);
-    // uncoarsen, src/uncoarsen.hpp:88-125
-    auto tr = clk::now();
-    Refiner<O, E, W> ref(eng, L0.n, (int64_t)L0.m, k);
-    ref.verbose = cfg.verbose;
-    part_t* cur_part = pa.p;
-    part_t* other = pb.p;
-    int nl = (int)levels.size();
-    if (st) st->num_levels = nl;
-    for (int l = nl - 1; l >= 0; l--) {
-        jet_level_stats_c cl = ref.refine(*levels[l], cur_part, cfg.imb, cfg.tol, cfg.ultra);
-        int idx = nl - 1 - l;
-        if (st && idx < JET_MAX_LEVELS) st->levels[idx] = cl;
-        if (l > 0) {
-            Level<O, E, W>& fine = *levels[l - 1];
-            k_project<O><<<grid_persistent(fine.n, 16), BLOCK, 0, s>>>(fine.n, levels[l]->map.p, cur_part, other); count_launch();
-            JET_LAUNCH_CHECK();
-            std::swap(cur_part, other);
-            if (l - 1 > 0) { levels[l].reset(); }
-        }
-    }
-    eng.sync();
-    meas[M_REFINE] += since(tr);
-    JET_CUDA(cudaMemcpyAsync(part_out, cur_part, sizeof(part_t) * L0.n, cudaMemcpyDeviceToDevice, s));
-    W cut_half = ref.best.cut / 2;
-    if (st) {
-        std::vector<W> hs(k);
-        JET_CUDA(cudaMemcpyAsync(hs.data(), ref.sizes_best.p, sizeof(W) * k, cudaMemcpyDeviceToHost, s));
-        eng.sync();
-        W largest = 0, smallest = ref.best.total_size;
-        for (W x : hs) { if (x > largest) largest = x; if (x < smallest) smallest = x; }
-        double opt = (double)(O)(((O)ref.best.total_size + k - 1) / k);
-        st->edge_cut = (int64_t)cut_half;
-        st->imb_ratio = (double)largest / opt;
-        st->largest_part = (int64_t)largest;
-        st->smallest_part = (int64_t)smallest;
-        st->coarsest_vertices = coarsest_n;
-        st->refine_iterations = ref.total_iters;
-        meas[M_COARSEN] = t_coarsen;
-        meas[M_TOTAL] = since(t_start);
-        for (int i = 0; i < JET_NUM_MEASUREMENTS; i++) st->measurements[i] = meas[i];
-    }
-    eng.sync();
-    return cut_half;
+    return uncoarsen_levels<O, E, W>(eng, cfg, levels, pa, pb, part_out, st, meas, t_start, t_coarsen, coarsest_n);
 }
 
 }  // namespace jetb
