@@ -62,6 +62,8 @@ NCU_TRAFFIC_RATIO = {
     "conn_build": {"grid3d128": {"ratio": (126.204928 + 62.770688) / 283.246592,
                                  "note": "ncu dram bytes of the finest-level launch (189.0 MB of 283.2 MB algorithmic), "
                                          "scaled to the per-launch average"}},
+    "conn_build_finest": {"grid3d128": {"ratio": (126.204928 + 62.770688) / 283.246592,
+                                        "note": "ncu dram bytes (read + write) of the finest-level launch"}},
 }
 ALG_NAME = {0: "2-hop matching", 1: "HEC", 2: "matching"}
 PART_FN = {"i32": "partition", "big": "partition_big", "biggest": "partition_biggest"}
@@ -386,7 +388,7 @@ def main():
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)
 
     for s in range(args.warmup):
-        part_fn(cfg, g, seed=100 + s, stream=stream)
+        part_fn(cfg, g, seed=1 + s % max(1, args.steps), stream=stream)
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
@@ -449,11 +451,14 @@ def main():
         pass
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    # dominant kernel class with an algorithmic byte model
+    # the table build of the finest level (a10, init_conn_data): the one
+    # kernel group of the hot path timed with CUDA events around its own
+    # launches inside the timed region; the class average over all levels
+    # is reported beside it
     ranked = sorted(((v["ms"], nm) for nm, v in prof.items() if v["bytes"] > 0 and v["launches"] > 0), reverse=True)
     roof = None
     if ranked:
-        nm = ranked[0][1]
+        nm = "conn_build_finest" if prof.get("conn_build_finest", {}).get("launches", 0) > 0 else ranked[0][1]
         v = prof[nm]
         per_launch_ms = v["ms"] / v["launches"]
         achieved = (v["bytes"] / v["launches"]) / (per_launch_ms / 1000.0) / 1e9
@@ -463,6 +468,12 @@ def main():
                 "traffic_note": NCU_TRAFFIC_RATIO.get(nm, {}).get(args.workload, {}).get("note"),
                 "bytes_per_launch": v["bytes"] / v["launches"], "ms_per_launch": per_launch_ms,
                 "launches": v["launches"]}
+        cb = prof.get("conn_build", {})
+        if cb.get("launches", 0) > 0 and nm != "conn_build":
+            roof["class_average_all_levels"] = {
+                "achieved": (cb["bytes"] / cb["launches"]) / (cb["ms"] / cb["launches"] / 1000.0) / 1e9,
+                "frac": (cb["bytes"] / cb["launches"]) / (cb["ms"] / cb["launches"] / 1000.0) / 1e9 / hbm_peak,
+                "launches": cb["launches"]}
     cpu_base = None
     if ws == 1 and not args.no_cpu_baseline:
         dt, ocut, oimb = oracle_partition(g, wl, seed=1)

@@ -252,8 +252,9 @@ int jet_device_ok(void);
 
 /* Kernel-class timing with CUDA events on the launching stream (used by the
  * benchmark).  kinds: 0 conn build, 1 LP select, 2 afterburner, 3 table
- * updates, 4 contraction, 5 heavy-edge proposal.  jet_prof_read fills
- * ms[6], bytes[6] (algorithmic bytes), launches[6]. */
+ * updates, 4 contraction, 5 heavy-edge proposal, 6 conn build of the finest
+ * level only.  jet_prof_read fills ms[7], bytes[7] (algorithmic bytes),
+ * launches[7]. */
 int jet_prof_enable(int on);
 int jet_prof_read(double* ms, double* bytes, int64_t* launches);
 

@@ -637,9 +637,9 @@ def prof_enable(on: bool = True):
 
 
 def prof_read():
-    ms = (ctypes.c_double * 6)()
-    by = (ctypes.c_double * 6)()
-    ln = (ctypes.c_int64 * 6)()
+    ms = (ctypes.c_double * 7)()
+    by = (ctypes.c_double * 7)()
+    ln = (ctypes.c_int64 * 7)()
     _check(load().jet_prof_read(ms, by, ln))
-    names = ["conn_build", "lp_select", "afterburn", "update", "contract", "coarsen_map"]
+    names = ["conn_build", "lp_select", "afterburn", "update", "contract", "coarsen_map", "conn_build_finest"]
     return {nm: dict(ms=ms[i], bytes=by[i], launches=ln[i]) for i, nm in enumerate(names)}

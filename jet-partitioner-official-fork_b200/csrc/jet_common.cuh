@@ -398,6 +398,7 @@ enum ProfKernel : int {
     PK_UPDATE,
     PK_CONTRACT,
     PK_HEC,
+    PK_CONN_FINEST,  // the table build of the finest level alone
     PK_COUNT
 };
 // Marks the start/end of a timed launch group.  bytes = algorithmic bytes.

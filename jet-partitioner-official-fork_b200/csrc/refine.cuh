@@ -2,8 +2,9 @@
 //
 // Connectivity tables: vertex i owns cap(i) = min(deg(i), k) slots starting at
 // coff[i]; the first csize[i] of them form an open-addressed table part ->
-// summed edge weight (home slot p % size, linear probing; direct-mapped when
-// size == k).  Slots are {part, weight} pairs so a probe and its update touch
+// summed edge weight (home slot slot_home(p, size, k), linear probing;
+// direct-mapped when size == k; the reference uses p % size, and only the
+// slot layout differs).  Slots are {part, weight} pairs so a probe and its update touch
 // one cache line.  Table sizes follow the reference exactly: built at cap,
 // shrunk to used + max(used/4, 3) when that is smaller, grown by appends when
 // an incremental insert finds no free slot.
@@ -20,6 +21,15 @@ struct Slot {
     part_t p;
     W v;
 };
+
+// Home slot of part p in a table of `size` slots: p itself when the table is
+// direct-mapped (size == k), else a multiplicative hash scaled to the size
+// (no division).  Only the slot layout depends on this choice, never a
+// table's contents or size.
+__host__ __device__ __forceinline__ part_t slot_home(part_t p, part_t size, part_t k) {
+    if (size == k) return p;
+    return (part_t)(((uint64_t)((uint32_t)p * 0x9E3779B1u) * (uint64_t)(uint32_t)size) >> 32);
+}
 
 __host__ __device__ __forceinline__ part_t shrunk_size(part_t used, part_t cap) {
     part_t q = used / 4;
@@ -86,28 +96,37 @@ struct RefArgs {
 };
 
 // ---------------------------------------------------------------- table build
-// deg <= 32: one thread per vertex, its distinct parts gathered in a private
-// 32-entry shared-memory set (interleaved so threads hit distinct banks).
+// Rows with dlo < deg <= dhi (dhi <= SET <= 32): one thread per vertex, its
+// distinct parts gathered in a private SET-entry shared-memory set
+// (interleaved so threads hit distinct banks; multiplicative hash into a
+// power-of-two set, no division).  Two instances cover deg <= 32: SET = 8
+// (256 threads, small enough for full occupancy) for deg <= 8 and SET = 32
+// for 8 < deg <= 32, launched only when the level has such rows.
 // Neighbours are read in batches of 8 with every load issued before the first
 // use, so a row costs about two memory latencies instead of two per entry.
 // The final table (at most 32 slots) is laid out with a register bitmask of
 // occupied slots and written once, with no read-back.
-template <class O, class E, class W>
-__global__ void __launch_bounds__(128) k_conn_thread(RefArgs<O, E, W> a, int only_marked, const int* gate) {
-    __shared__ part_t sk[32][128];
-    __shared__ W sv[32][128];
+template <int SET>
+__device__ __forceinline__ int set_home(part_t p) {
+    constexpr int bits = SET == 8 ? 3 : (SET == 16 ? 4 : 5);
+    return (int)(((uint32_t)p * 0x9E3779B1u) >> (32 - bits));
+}
+
+template <int SET, int THREADS, class O, class E, class W>
+__global__ void __launch_bounds__(THREADS) k_conn_thread(RefArgs<O, E, W> a, int dlo, int dhi, int only_marked, const int* gate) {
+    __shared__ part_t sk[SET][THREADS];
+    __shared__ W sv[SET][THREADS];
     if (gate && !*gate) return;
     const int t = threadIdx.x;
     for (int64_t x = blockIdx.x * (int64_t)blockDim.x + t; x < a.g.n; x += (int64_t)gridDim.x * blockDim.x) {
         O i = (O)x;
         E rs = a.g.row[i], re = a.g.row[i + 1];
         E deg = re - rs;
-        if (deg > THREAD_DEG) continue;
+        if (deg <= dlo || deg > dhi) continue;
         if (only_marked && !a.mark[i]) continue;
-        const int sz = (int)deg;  // set capacity: at most deg distinct parts
-        for (int s = 0; s < sz; s++) sk[s][t] = NULL_PART;
+#pragma unroll
+        for (int s = 0; s < SET; s++) sk[s][t] = NULL_PART;
         int used = 0;
-        bool ok = true;
         for (E j0 = rs; j0 < re; j0 += 8) {
             O vb[8];
             W wb[8];
@@ -121,11 +140,10 @@ __global__ void __launch_bounds__(128) k_conn_thread(RefArgs<O, E, W> a, int onl
 #pragma unroll
             for (int u = 0; u < 8; u++) {
                 part_t p = pb[u];
-                if (p == NULL_PART || !ok) continue;
-                int h = p % sz;
-                int guard = 0;
-                while (sk[h][t] != NULL_PART && sk[h][t] != p && ++guard <= sz) h = h + 1 == sz ? 0 : h + 1;
-                if (guard > sz) { ok = false; continue; }
+                if (p == NULL_PART) continue;
+                int h = set_home<SET>(p);
+                // at most deg <= SET distinct parts: a free or matching slot is always found
+                while (sk[h][t] != NULL_PART && sk[h][t] != p) h = (h + 1) & (SET - 1);
                 if (sk[h][t] == NULL_PART) { sk[h][t] = p; sv[h][t] = wb[u]; used++; }
                 else sv[h][t] += wb[u];
             }
@@ -134,17 +152,19 @@ __global__ void __launch_bounds__(128) k_conn_thread(RefArgs<O, E, W> a, int onl
         part_t size = cap == 0 ? 0 : shrunk_size(used, cap);
         Slot<W>* base = a.slots + a.coff[i];
         uint32_t occ = 0;  // size <= cap <= 32
-        for (int s = 0; ok && s < sz; s++) {
+        bool ok = true;
+#pragma unroll
+        for (int s = 0; s < SET; s++) {
             part_t p = sk[s][t];
-            if (p == NULL_PART) continue;
-            int po = p % size;
+            if (p == NULL_PART || !ok) continue;
+            int po = slot_home(p, size, a.k);
             if (size < a.k) {
                 int guard = 0;
                 while ((occ >> po) & 1u) {
                     po = po + 1 == size ? 0 : po + 1;
                     if (++guard > size) { ok = false; break; }
                 }
-                if (!ok) break;
+                if (!ok) continue;
             }
             occ |= 1u << po;
             Slot<W> sl;
@@ -172,7 +192,7 @@ __global__ void __launch_bounds__(128) k_conn_thread(RefArgs<O, E, W> a, int onl
 template <class W>
 __device__ __forceinline__ bool smem_table_add(part_t* keys, W* vals, part_t cap, part_t k, part_t p, W w, int* err) {
     volatile part_t* vk = keys;
-    part_t po = p % cap;
+    part_t po = slot_home(p, cap, k);
     bool claimed = false;
     if (cap == k) {
         if (vk[po] == NULL_PART && atomicCAS((int*)&keys[po], NULL_PART, p) == NULL_PART) claimed = true;
@@ -211,7 +231,7 @@ __device__ __forceinline__ void smem_table_flush(const part_t* keys, const W* va
         for (int s = tid; s < cap; s += nt) {
             part_t p = keys[s];
             if (p == NULL_PART) continue;
-            part_t po = p % size;
+            part_t po = slot_home(p, size, k);
             int guard = 0;
             bool placed = true;
             while (true) {
@@ -288,12 +308,14 @@ __global__ void __launch_bounds__(1024) k_conn_cta(RefArgs<O, E, W> a, const O* 
 
 // ---------------------------------------------------------------- lookups
 template <class W>
-__device__ __forceinline__ W table_lookup(const Slot<W>* base, part_t target, part_t size) {  // src/jet_refiner.hpp:891-901
+__device__ __forceinline__ W table_lookup(const Slot<W>* base, part_t target, part_t size, part_t k) {  // src/jet_refiner.hpp:891-901
+    if (size <= 0) return 0;
+    part_t pi = slot_home(target, size, k);
     for (part_t q = 0; q < size; q++) {
-        part_t pi = (target + q) % size;
         part_t e = base[pi].p;
         if (e == target) return base[pi].v;
         if (e == NULL_PART) return 0;
+        pi = pi + 1 == size ? 0 : pi + 1;
     }
     return 0;
 }
@@ -948,7 +970,7 @@ __device__ __forceinline__ void d_apply_moves(RefArgs<O, E, W> a, int hist) {
         part_t p = a.part[i], b = a.dest[i];
         const Slot<W>* base = a.slots + a.coff[i];
         part_t sz = a.csize[i];
-        c1 += table_lookup<W>(base, b, sz) - table_lookup<W>(base, p, sz);
+        c1 += table_lookup<W>(base, b, sz, a.k) - table_lookup<W>(base, p, sz, a.k);
         a.dest_cache[i] = NULL_PART;
         W w = a.g.vw[i];
         if (hist) { atomic_add(&hs[p], -w); atomic_add(&hs[b], w); }
@@ -973,7 +995,7 @@ template <class O, class E, class W>
 __device__ __forceinline__ void conn_sub(const RefArgs<O, E, W>& a, O v, part_t p, W w) {
     Slot<W>* base = a.slots + a.coff[v];
     part_t vsize = a.csize[v];
-    part_t po = p % vsize;
+    part_t po = slot_home(p, vsize, a.k);
     part_t guard = 0;
     while (ld_cg(&base[po].p) != p) {
         po = po + 1 == vsize ? 0 : po + 1;
@@ -990,26 +1012,27 @@ __device__ __forceinline__ void conn_add(const RefArgs<O, E, W>& a, O v, part_t 
     E vs = a.coff[v];
     Slot<W>* base = a.slots + vs;
     part_t vsize = ld_cg(&a.csize[v]);
-    part_t po = best % vsize;
+    const part_t home = slot_home(best, vsize, a.k);
+    part_t po = home;
     bool success = false;
-    for (part_t q = 0; q < vsize; q++) {
-        part_t pi = (best + q) % vsize;
+    for (part_t q = 0, pi = home; q < vsize; q++) {
         part_t e = ld_cg(&base[pi].p);
         if (e == best) { success = true; po = pi; break; }
         else if (e == NULL_PART) break;
+        pi = pi + 1 == vsize ? 0 : pi + 1;
     }
     part_t count = 0;
     while (!success && count < vsize) {
         part_t px = ld_cg(&base[po].p);
         while (px != best && px > NULL_PART && count++ < vsize) {
-            po = (po + 1) % vsize;
+            po = po + 1 == vsize ? 0 : po + 1;
             px = ld_cg(&base[po].p);
         }
         if (px == best) success = true;
         else if (px <= NULL_PART) {
             part_t old = atomicCAS((int*)&base[po].p, px, best);
             if (old == best || old <= NULL_PART) success = true;
-            else { po = (po + 1) % vsize; count++; }
+            else { po = po + 1 == vsize ? 0 : po + 1; count++; }
         }
     }
     if (!success) {
@@ -1107,7 +1130,7 @@ __device__ __forceinline__ void d_cut_after(RefArgs<O, E, W> a) {
         O i = a.moves[x];
         const Slot<W>* base = a.slots + a.coff[i];
         part_t sz = a.csize[i];
-        c2 += table_lookup<W>(base, a.part[i], sz) - table_lookup<W>(base, a.dest[i], sz);
+        c2 += table_lookup<W>(base, a.part[i], sz, a.k) - table_lookup<W>(base, a.dest[i], sz, a.k);
     }
     c2 = group_sum<W>(c2, 32);
     if ((threadIdx.x & 31) == 0 && c2) atomic_add(&a.dev->cut2, c2);

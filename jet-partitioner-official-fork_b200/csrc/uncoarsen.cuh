@@ -134,7 +134,10 @@ struct Refiner {
         auto a = args(L);
         if (cta_smem() > (size_t)device_info().max_smem_optin - 1024)
             throw JetError{JET_ERR_INVALID, "num_parts too large for the shared-memory connectivity tables"};
-        k_conn_thread<O, E, W><<<grid_persistent(L.n, 16), 128, 0, s>>>(a, only_marked, gate); count_launch();
+        k_conn_thread<8, 256, O, E, W><<<grid_persistent(L.n, 8), 256, 0, s>>>(a, -1, 8, only_marked, gate); count_launch();
+        if (L.max_deg > 8) {
+            k_conn_thread<32, 128, O, E, W><<<grid_persistent(L.n, 16), 128, 0, s>>>(a, 8, THREAD_DEG, only_marked, gate); count_launch();
+        }
         JET_LAUNCH_CHECK();
         if (L.n_warp > 0) {
             if (k <= WARP_TABLE) {
@@ -153,14 +156,18 @@ struct Refiner {
     // init_conn_data, src/jet_refiner.hpp:958-1048.  Returns sum of capacities.
     int64_t init_conn(const Level<O, E, W>& L) {
         exclusive_scan<E, GetConnCap<O, E>>(GetConnCap<O, E>{L.row, k}, L.n, coff.p, coff.p + L.n, e.scan, s);
-        int h = prof_begin(s);
-        build_tables(L, 0, nullptr);
-        E C = 0;
         JET_CUDA(cudaMemcpyAsync(&e.hscal[0], coff.p + L.n, sizeof(E), cudaMemcpyDeviceToHost, s));
         e.sync();
-        C = *(E*)&e.hscal[0];
-        prof_end(h, PK_CONN_BUILD,
-                 (double)L.n * (3 * sizeof(E) + 4) + (double)L.m * (sizeof(O) + sizeof(W) + 4) + (double)C * sizeof(Slot<W>), s);
+        E C = *(E*)&e.hscal[0];
+        // events bracket exactly the table-build kernels
+        const double bytes =
+            (double)L.n * (3 * sizeof(E) + 4) + (double)L.m * (sizeof(O) + sizeof(W) + 4) + (double)C * sizeof(Slot<W>);
+        const bool finest = (int64_t)L.n == (int64_t)n_max;
+        int h = prof_begin(s);
+        int hf = finest ? prof_begin(s) : -1;
+        build_tables(L, 0, nullptr);
+        if (finest) prof_end(hf, PK_CONN_FINEST, bytes, s);
+        prof_end(h, PK_CONN_BUILD, bytes, s);
         fill<part_t>(dest_cache.p, L.n, NULL_PART, s);
         JET_CUDA(cudaMemsetAsync(lock.p, 0, L.n, s));
         return (int64_t)C;
