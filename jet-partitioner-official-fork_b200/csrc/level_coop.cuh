@@ -297,6 +297,7 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             default: d_update_small<32, true, O, E, W>(a); d_mark_neighbors<32, O, E, W>(a); break;
         }
         d_update_small_hub<true, O, E, W>(a);
+        d_mark_neighbors_hub<O, E, W>(a);
         if (!level_sync<CL>(cs.bar, err)) return;
         if (a.dev->large) {
             // update_large: queue the marked rows (one coalesced pass), then

@@ -178,6 +178,7 @@ k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, 
             default: d_update_small<32, true, O, E, W>(a); d_mark_neighbors<32, O, E, W>(a); break;
         }
         d_update_small_hub<true, O, E, W>(a);
+        d_mark_neighbors_hub<O, E, W>(a);
         __syncthreads();
         d_conn_warp<O, E, W>(a, nullptr, n, 1, &a.dev->large);  // update_large: rebuild marked rows
         __syncthreads();

@@ -246,10 +246,38 @@ __device__ __forceinline__ void smem_table_flush(const part_t* keys, const W* va
     if (tid == 0) *size_out = size;
 }
 
+// Adds edges rs+t, rs+t+nt, ... of a row into a shared-memory table; four
+// edges per thread per round with every load issued before the first use
+// (the part gather depends on the neighbour id load).  Returns the slots this
+// thread claimed.
+template <class O, class E, class W>
+__device__ __forceinline__ int table_add_edges(const RefArgs<O, E, W>& a, part_t* keys, W* vals, part_t cap, E rs, E re, int t,
+                                               int nt) {
+    int mine = 0;
+    for (E j0 = rs + t; j0 < re; j0 += 4 * (E)nt) {
+        O v[4];
+        W w[4];
+        part_t p[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            E j = j0 + (E)u * nt;
+            v[u] = j < re ? a.g.adj[j] : (O)0;
+            w[u] = j < re ? a.g.val[j] : (W)0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) p[u] = j0 + (E)u * nt < re ? a.part[v[u]] : NULL_PART;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (p[u] != NULL_PART) mine += smem_table_add<W>(keys, vals, cap, a.k, p[u], w[u], &a.dev->err);
+    }
+    return mine;
+}
+
 // 32 < deg <= 4096 and k <= WARP_TABLE: one warp per vertex, table in shared memory.
 static constexpr int WARP_TABLE = 512;
 template <class O, class E, class W>
-__device__ __forceinline__ void d_conn_warp(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) {
+__device__ __forceinline__ void d_conn_warp(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate,
+                                            int64_t max_deg = INT64_MAX) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     if (gate && !*gate) return;
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -262,11 +290,12 @@ __device__ __forceinline__ void d_conn_warp(RefArgs<O, E, W> a, const O* list, O
         O i = list ? list[x] : (O)x;  // no list: every vertex
         if (only_marked && !a.mark[i]) continue;
         E rs = a.g.row[i], re = a.g.row[i + 1];
+        if ((int64_t)(re - rs) > max_deg) continue;  // left to the CTA-per-row kernel
         part_t cap = conn_cap<E>(re - rs, a.k);
         for (int s = lane; s < cap; s += 32) { keys[s] = NULL_PART; vals[s] = 0; }
         __syncwarp();
         int mine = 0;
-        for (E j = rs + lane; j < re; j += 32) mine += smem_table_add<W>(keys, vals, cap, a.k, a.part[a.g.adj[j]], a.g.val[j], &a.dev->err);
+        mine += table_add_edges<O, E, W>(a, keys, vals, cap, rs, re, lane, 32);
         __syncwarp();
         int used = group_sum<int>(mine, 32);
         smem_table_flush<W>(keys, vals, cap, used, a.k, a.slots + a.coff[i], &a.csize[i], lane, 32, false, &a.dev->err);
@@ -275,11 +304,15 @@ __device__ __forceinline__ void d_conn_warp(RefArgs<O, E, W> a, const O* list, O
     }
 }
 template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_conn_warp(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) { d_conn_warp<O, E, W>(a, list, count, only_marked, gate); }
+__global__ void __launch_bounds__(BLOCK) k_conn_warp(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate,
+                                                     int64_t max_deg) {
+    d_conn_warp<O, E, W>(a, list, count, only_marked, gate, max_deg);
+}
 
 // Any degree: one CTA per vertex, table of cap <= k slots in shared memory.
 template <class O, class E, class W>
-__device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) {
+__device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate,
+                                           int64_t min_deg = 0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_used;
     if (gate && !*gate) return;
@@ -288,13 +321,14 @@ __device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O 
     for (O x = blockIdx.x; x < count; x += gridDim.x) {
         O i = list[x];
         if (only_marked && !a.mark[i]) continue;
+        if ((int64_t)(a.g.row[i + 1] - a.g.row[i]) <= min_deg) continue;  // done by the warp kernel
         E rs = a.g.row[i], re = a.g.row[i + 1];
         part_t cap = conn_cap<E>(re - rs, a.k);
         for (int s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = NULL_PART; vals[s] = 0; }
         if (threadIdx.x == 0) s_used = 0;
         __syncthreads();
         int mine = 0;
-        for (E j = rs + threadIdx.x; j < re; j += blockDim.x) mine += smem_table_add<W>(keys, vals, cap, a.k, a.part[a.g.adj[j]], a.g.val[j], &a.dev->err);
+        mine += table_add_edges<O, E, W>(a, keys, vals, cap, rs, re, threadIdx.x, blockDim.x);
         mine = group_sum<int>(mine, 32);
         if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&s_used, mine);
         __syncthreads();
@@ -304,7 +338,10 @@ __device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O 
     }
 }
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate) { d_conn_cta<O, E, W>(a, list, count, only_marked, gate); }
+__global__ void __launch_bounds__(1024) k_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate,
+                                                   int64_t min_deg) {
+    d_conn_cta<O, E, W>(a, list, count, only_marked, gate, min_deg);
+}
 
 // ---------------------------------------------------------------- lookups
 template <class W>
@@ -1108,10 +1145,12 @@ __device__ __forceinline__ void d_mark_neighbors(RefArgs<O, E, W> a) {
     {                                                                                       \
         if (in) {                                                                           \
             O i = a.moves[x];                                                               \
-            for (E j = a.g.row[i] + lane; j < a.g.row[i + 1]; j += G) {                     \
-                O v = a.g.adj[j];                                                           \
-                if (!a.mark[v]) a.mark[v] = 1;                                              \
-            }                                                                               \
+            E rs = a.g.row[i], re = a.g.row[i + 1];                                         \
+            if (re - rs <= HUB_DEG)  /* hubs: one CTA each (d_mark_neighbors_hub) */         \
+                for (E j = rs + lane; j < re; j += G) {                                     \
+                    O v = a.g.adj[j];                                                       \
+                    if (!a.mark[v]) a.mark[v] = 1; /* read first: few lines get dirtied */  \
+                }                                                                           \
         }                                                                                   \
     }
     JET_GROUP_LOOP(G, count, MARK_BODY)
@@ -1119,6 +1158,21 @@ __device__ __forceinline__ void d_mark_neighbors(RefArgs<O, E, W> a) {
 }
 template <int G, class O, class E, class W>
 __global__ void __launch_bounds__(BLOCK) k_mark_neighbors(RefArgs<O, E, W> a) { d_mark_neighbors<G, O, E, W>(a); }
+
+template <class O, class E, class W>
+__device__ __forceinline__ void d_mark_neighbors_hub(RefArgs<O, E, W> a) {
+    if (!a.dev->large) return;
+    O count = a.dev->nmoves_hub;
+    for (O x = blockIdx.x; x < count; x += gridDim.x) {
+        O i = a.moves_hub[x];
+        for (E j = a.g.row[i] + threadIdx.x; j < a.g.row[i + 1]; j += blockDim.x) {
+            O v = a.g.adj[j];
+            if (!a.mark[v]) a.mark[v] = 1;
+        }
+    }
+}
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_mark_neighbors_hub(RefArgs<O, E, W> a) { d_mark_neighbors_hub<O, E, W>(a); }
 
 // perform_moves part 2 (src/jet_refiner.hpp:937-946): cut change from the
 // updated tables.

@@ -141,17 +141,28 @@ struct Refiner {
         JET_LAUNCH_CHECK();
         if (L.n_warp > 0) {
             if (k <= WARP_TABLE) {
-                k_conn_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, warp_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate); count_launch();
+                k_conn_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, warp_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate, INT64_MAX); count_launch();
             } else {
-                k_conn_cta<O, E, W><<<grid_for(L.n_warp, 1) < 4096 ? grid_for(L.n_warp, 1) : 4096, 256, cta_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate); count_launch();
+                k_conn_cta<O, E, W><<<grid_for(L.n_warp, 1) < 4096 ? grid_for(L.n_warp, 1) : 4096, 256, cta_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate, 0); count_launch();
             }
             JET_LAUNCH_CHECK();
         }
         if (L.n_hub > 0) {
-            k_conn_cta<O, E, W><<<grid_for(L.n_hub, 1) < 4096 ? grid_for(L.n_hub, 1) : 4096, 1024, cta_smem(), s>>>(a, L.hub_list.p, L.n_hub, only_marked, gate); count_launch();
+            // rows of the hub bin up to WARP_ROW_MAX edges still go one warp
+            // per row (thousands of warps beat one CTA per row on dense levels);
+            // only the longest rows get a whole CTA
+            int64_t cta_from = 0;
+            if (k <= WARP_TABLE) {
+                k_conn_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, warp_smem(), s>>>(a, L.hub_list.p, L.n_hub, only_marked, gate, WARP_ROW_MAX); count_launch();
+                cta_from = WARP_ROW_MAX;
+            }
+            if ((int64_t)L.max_deg > cta_from) {
+                k_conn_cta<O, E, W><<<grid_for(L.n_hub, 1) < 4096 ? grid_for(L.n_hub, 1) : 4096, 1024, cta_smem(), s>>>(a, L.hub_list.p, L.n_hub, only_marked, gate, cta_from); count_launch();
+            }
             JET_LAUNCH_CHECK();
         }
     }
+    static constexpr int64_t WARP_ROW_MAX = 16384;
 
     // init_conn_data, src/jet_refiner.hpp:958-1048.  Returns sum of capacities.
     int64_t init_conn(const Level<O, E, W>& L) {
@@ -293,6 +304,7 @@ struct Refiner {
             // the subtract pass must finish before any add: two launches
             k_update_small_hub<false, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch();
             k_update_small_hub<true, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch();
+            k_mark_neighbors_hub<O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch();
             JET_LAUNCH_CHECK();
         }
         build_tables(L, 1, &dev.p->large);
