@@ -134,11 +134,22 @@ __device__ __forceinline__ uint32_t slot_hash(uint64_t k) {
 }
 
 // Walks the concatenated adjacency of a coarse row's members with the whole
-// CTA: members are taken blockDim at a time, their degrees prefix-summed in
-// shared memory, and each thread locates its edge by binary search.
+// CTA.  A row of at most FEW_MEMBERS members (a matched pair or a singleton) is
+// walked member by member with the CTA striding over each member's edges;
+// otherwise members are taken blockDim at a time, their degrees
+// prefix-summed in shared memory, and each thread locates its edge by binary
+// search.  The row's member count is CTA-uniform, so is the choice.
+static constexpr int FEW_MEMBERS = 2;
 template <int THREADS, class O, class E, class W, class F>
 __device__ __forceinline__ void cta_for_row_edges(GView<O, E, W> g, const O* members, O m0, O m1, E* s_pref, O* s_mem,
                                                   F&& f) {
+    if (m1 - m0 <= FEW_MEMBERS) {
+        for (O mi = m0; mi < m1; mi++) {
+            O i = members[mi];
+            for (E j = g.row[i] + threadIdx.x; j < g.row[i + 1]; j += THREADS) f(j);
+        }
+        return;
+    }
     for (O mb = m0; mb < m1; mb += THREADS) {
         O cnt = m1 - mb < THREADS ? m1 - mb : THREADS;
         E d = 0;
