@@ -90,6 +90,14 @@ class ClockSampler:
             self.out = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.gpu)], stdout=self.out, stderr=subprocess.DEVNULL)
+            # wait for the first sample: nvidia-smi's start-up (NVML
+            # initialisation) must not overlap the timed region
+            t0 = time.time()
+            while time.time() - t0 < 15 and self.proc.poll() is None:
+                self.out.flush()
+                if os.path.getsize(self.path) > 0:
+                    break
+                time.sleep(0.05)
         except Exception:
             self.proc = None
 
@@ -132,30 +140,60 @@ def oracle_partition(g, wl, seed):
     return time.perf_counter() - t, cut, st.imb
 
 
+_REF_STATE = {}
+
+
+def _ref_init(workload):
+    """Worker set-up for the CPU arm: the workload's graph in the oracle's form."""
+    jet = load_pkg()
+    wl = WORKLOADS[workload]
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    g = wl["make"](jet.graphs, "cpu")
+    _REF_STATE.update(og=oracle.G.from_csr(g), oracle=oracle, wl=wl)
+
+
+def _ref_partition(seed):
+    st = _REF_STATE
+    t = time.perf_counter()
+    part, cut, info = st["oracle"].partition(st["og"], st["wl"]["k"], alg=st["wl"]["alg"], imb=st["wl"]["imb"], seed=seed)
+    return time.perf_counter() - t, cut, info.imb
+
+
 def run_reference(args, wl, rank):
-    """CPU oracle of the reference algorithm, one full partition per step."""
+    """CPU arm: the oracle (a restatement of the reference's algorithm; the
+    reference itself needs Kokkos and cannot be built here) on every host
+    core, one independent partition per core per step (one graph is
+    partitioned by one thread, so the cores run replicas with different
+    seeds); graphs/s = partitions finished / wall time."""
     if rank != 0:
         return
+    import multiprocessing as mp
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
     jet = load_pkg()
     g = wl["make"](jet.graphs, "cpu")
-    for s in range(args.warmup):
-        oracle_partition(g, wl, seed=100 + s)
-    times, cuts, imbs = [], [], []
-    for s in range(args.steps):
-        dt, cut, imb = oracle_partition(g, wl, seed=1 + s)
-        times.append(dt)
-        cuts.append(cut)
-        imbs.append(imb)
-    total = sum(times)
-    value = args.steps / total
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_ref_init, initargs=(args.workload,)) as pool:
+        for s in range(args.warmup):
+            pool.map(_ref_partition, [100 + s * cores + c for c in range(cores)])
+        walls, cuts, imbs = [], [], []
+        for s in range(args.steps):
+            t = time.perf_counter()
+            res = pool.map(_ref_partition, [1 + s * cores + c for c in range(cores)])
+            walls.append(time.perf_counter() - t)
+            cuts += [r[1] for r in res]
+            imbs += [r[2] for r in res]
+    total = sum(walls)
+    value = args.steps * cores / total
     line = {
         "impl": "reference", "metric": "graphs/sec", "value": value, "unit": "graphs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": wl["tier"], "data": "synthetic",
         "config": config_of(args, wl, g),
         "edges_per_s": value * g.nnz / 2, "cut_median": statistics.median(cuts), "imbalance_max": max(imbs),
-        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": 1, "kind": "port",
-                         "sample": "%d full partitions of the workload on one host thread (oracle/jet_oracle.cpp)" % args.steps},
+        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": cores, "kind": "port",
+                         "sample": "%d steps of %d concurrent full partitions (one per host core, oracle/jet_oracle.cpp)"
+                                   % (args.steps, cores)},
         "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -268,6 +306,39 @@ def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None):
             "timing": "wall clock, device synchronised before and after; max over ranks"}
 
 
+def run_powerlaw(jet, dev, scale, steps=2):
+    """The power-law config: R-MAT 2^scale (edge factor 8, symmetrised,
+    de-duplicated, unit weights), int64 offsets and weights, 2-hop matching,
+    k = 256, imbalance 1.10.  One warm-up and `steps` timed partitions with
+    the graph resident in HBM (CUDA events); edges/s per phase is the sum of
+    the level edge counts over the phase's time."""
+    import torch
+    g = jet.graphs.rmat(scale, 8, seed=1, tier="big", device=dev)
+    cfg = jet.config_t(coarsening_alg=0, num_parts=256, max_imb_ratio=1.10)
+    jet.partition_big(cfg, g, seed=1)
+    torch.cuda.synchronize()
+    times, last = [], None
+    for s in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        part, cut, exp = jet.partition_big(cfg, g, seed=1 + s)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+        last = (cut, exp)
+    cut, exp = last
+    m = {k: v for k, v in zip(jet.MEASUREMENT_NAMES, exp.measurements)}
+    sum_m = sum(cl.numEdges for cl in exp.coarseLevels) / 2
+    return {"workload": "rmat%d" % scale, "n": g.n, "undirected_edges": g.nnz // 2, "k": 256, "coarsening": "2-hop matching",
+            "imbalance": 1.10, "tier": "big", "ms_per_partition": statistics.median(times), "steps": steps,
+            "edges_per_s": (g.nnz / 2) / (statistics.median(times) / 1000.0), "cut": cut, "imbalance_ratio": exp.imb_ratio,
+            "levels": len(exp.coarseLevels),
+            "phase_ms": {"coarsen": 1000 * m["coarsen"], "initial_partition": 1000 * m["initial-partition"],
+                         "refine": 1000 * m["refine"]},
+            "refine_level_edges_per_s": sum_m / max(m["refine"], 1e-9)}
+
+
 def serving_workload(jet, dev, count, seed=5):
     """Requests mixing 2D grids, random geometric graphs and R-MAT graphs:
     n log-uniform in [1e4, 1e6], mean degree in [6, 16], k in {16..256}."""
@@ -355,6 +426,7 @@ def main():
     ap.add_argument("--batched", type=int, default=512, help="graphs in the batched comparison (0 = skip)")
     ap.add_argument("--serving", type=int, default=96, help="requests in the serving run (0 = skip)")
     ap.add_argument("--workers", type=int, default=16)
+    ap.add_argument("--powerlaw-scale", type=int, default=24, help="R-MAT scale of the power-law run (0 = skip)")
     ap.add_argument("--only", default=None, choices=["conn_build"],
                     help="time one kernel alone on the workload's finest graph (profiling case)")
     args = ap.parse_args()
@@ -387,8 +459,11 @@ def main():
     torch.cuda.set_stream(stream)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)
 
+    # timed steps reuse the warm-up seeds (every step is a full partition;
+    # this only keeps the set of buffer sizes seen in the timed region warm)
+    nseeds = max(1, min(args.warmup, args.steps))
     for s in range(args.warmup):
-        part_fn(cfg, g, seed=1 + s % max(1, args.steps), stream=stream)
+        part_fn(cfg, g, seed=1 + s % nseeds, stream=stream)
     torch.cuda.synchronize()
     if ws > 1:
         dist.barrier()
@@ -403,7 +478,7 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        part, cut, exp = part_fn(cfg, g, seed=1 + s, stream=stream)
+        part, cut, exp = part_fn(cfg, g, seed=1 + s % nseeds, stream=stream)
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
@@ -438,6 +513,7 @@ def main():
     e2e_value = ws * len(e2e_times) / sum(e2e_times) if e2e_times else None
     batched = run_batched(jet, dev, args.batched, args.workers, ws, rank, dist) if args.batched > 0 else None
     serving = run_serving(jet, dev, args.serving, args.workers, 120 << 30) if args.serving > 0 and rank == 0 else None
+    powerlaw = run_powerlaw(jet, dev, args.powerlaw_scale) if args.powerlaw_scale > 0 and rank == 0 else None
 
     if rank != 0:
         if ws > 1:
@@ -493,6 +569,7 @@ def main():
         "cpu_baseline": cpu_base,
         "batched": batched,
         "serving": serving,
+        "powerlaw": powerlaw,
         "clocks": clk,
         "gpu_launches": launches,
     }

@@ -168,6 +168,7 @@ struct Dev {
     int sms = 148;
     int max_smem_optin = 227 * 1024;
     int coop = 0;  // cooperative launches supported
+    size_t total_mem = (size_t)180 << 30;
 };
 Dev& device_info();
 

@@ -38,6 +38,7 @@ Dev& device_info() {
             d.sms = p.multiProcessorCount;
             d.max_smem_optin = (int)p.sharedMemPerBlockOptin;
             d.coop = p.cooperativeLaunch;
+            d.total_mem = p.totalGlobalMem;
         }
         cached_dev = dev;
     }
@@ -96,9 +97,14 @@ void* big_alloc(size_t bytes, cudaStream_t s, size_t* got) {
             return b.p;
         }
     }
+    // round up to one of four size classes per power of two, so that later
+    // requests of similar size find this block in the cache
+    size_t cls = (size_t)1 << (63 - __builtin_clzll((unsigned long long)bytes));
+    size_t step = cls / 4;
+    size_t want = (bytes + step - 1) / step * step;
     void* p = nullptr;
-    JET_CUDA(cudaMallocFromPoolAsync(&p, bytes, pool_for_current_device(), s));
-    *got = bytes;
+    JET_CUDA(cudaMallocFromPoolAsync(&p, want, pool_for_current_device(), s));
+    *got = want;
     return p;
 }
 
@@ -113,9 +119,10 @@ void big_free(void* p, size_t bytes, cudaStream_t s) {
     std::lock_guard<std::mutex> lk(g_big_mu);
     g_big_free.push_back({p, bytes, dev, ev});
     g_big_cached += bytes;
-    // keep at most a quarter of this device's memory cached; oldest blocks go first
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
+    // keep at most a quarter of this device's memory cached; oldest blocks go
+    // first (the device size comes from the cached properties: querying free
+    // memory here stalled for tens of milliseconds)
+    const size_t total_b = device_info().total_mem;
     size_t mine = 0;
     for (const BigBlock& b : g_big_free) if (b.dev == dev) mine += b.bytes;
     for (size_t i = 0; i < g_big_free.size() && mine > total_b / 4;) {

@@ -996,11 +996,15 @@ W run_partition(Engine<O, E, W>& eng, const Cfg& cfg, const GraphIn<O, E, W>& in
         levels.push_back(std::move(next));
         if (levels.size() > 200) break;
     }
+    double t_rel0 = since(t_start);
     skey.release();
     sval.release();
+    double t_rel1 = since(t_start);
     eng.sync();
     double t_coarsen = since(t_start);
-    if (debug_timing()) fprintf(stderr, "jet: coarsening done %.3f ms\n", t_coarsen * 1e3);
+    if (debug_timing())
+        fprintf(stderr, "jet: coarsening done %.3f ms (loop end %.3f, after release %.3f)\n", t_coarsen * 1e3, t_rel0 * 1e3,
+                t_rel1 * 1e3);
     // initial partition
     auto ti = clk::now();
     Level<O, E, W>& coarsest = *levels.back();
