@@ -185,7 +185,7 @@ __device__ __forceinline__ void cta_for_row_edges(GView<O, E, W> g, const O* mem
 template <int THREADS, int SLOTS, class O, class E, class W>
 __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, const O* map, const O* list, const O* count,
                                                           const O* moff, const O* members, const E* hrow, O* skey, W* sval,
-                                                          O* ucnt) {
+                                                          O* ucnt, O nc) {
     extern __shared__ __align__(16) unsigned char ct_smem[];
     O* keys = (O*)ct_smem;
     W* vals = (W*)(ct_smem + align16((size_t)SLOTS * sizeof(O)));
@@ -194,6 +194,7 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
     __shared__ E s_pref[THREADS];
     __shared__ O s_mem[THREADS];
     __shared__ int s_cnt;
+    __shared__ int s_sw[32];
     O total_rows = *count;
     for (O x = blockIdx.x; x < total_rows; x += gridDim.x) {
         O c = list[x];
@@ -238,12 +239,41 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
         }
         __syncthreads();
         int u = s_cnt;
-        int P = 1;
-        while (P < u) P <<= 1;
-        for (int i = u + threadIdx.x; i < P; i += THREADS) sk[i] = std::numeric_limits<O>::max();
-        __syncthreads();
-        block_bitonic_sort<THREADS>(sk, sv, P);
-        for (int i = threadIdx.x; i < u; i += THREADS) { skey[hs + i] = sk[i]; sval[hs + i] = sv[i]; }
+        const int64_t words = ((int64_t)nc + 31) >> 5;
+        if (words * 8 <= (int64_t)(align16((size_t)SLOTS * sizeof(O)) + (size_t)SLOTS * sizeof(W))) {
+            // Rank by bitmap: the row's distinct ids set bits in an nc-bit
+            // map (in the freed hash-table space); an id's rank is the number
+            // of set bits before it (per-word prefix counts + popcount), so the
+            // row is written in id order with no comparison sort.
+            uint32_t* bm = (uint32_t*)ct_smem;
+            int* wpre = (int*)(bm + words);
+            for (int64_t w = threadIdx.x; w < words; w += THREADS) bm[w] = 0;
+            __syncthreads();
+            for (int e = threadIdx.x; e < u; e += THREADS) atomicOr(&bm[sk[e] >> 5], 1u << (sk[e] & 31));
+            __syncthreads();
+            const int per = (int)((words + THREADS - 1) / THREADS);
+            const int64_t w0 = (int64_t)threadIdx.x * per, w1 = w0 + per < words ? w0 + per : words;
+            int cntb = 0;
+            for (int64_t w = w0; w < w1; w++) cntb += __popc(bm[w]);
+            int totb;
+            int run = block_exclusive_scan<int>(cntb, s_sw, totb);
+            for (int64_t w = w0; w < w1; w++) { wpre[w] = run; run += __popc(bm[w]); }
+            __syncthreads();
+            for (int e = threadIdx.x; e < u; e += THREADS) {
+                O key = sk[e];
+                int64_t w = key >> 5;
+                int r = wpre[w] + __popc(bm[w] & ((1u << (key & 31)) - 1u));
+                skey[hs + r] = key;
+                sval[hs + r] = sv[e];
+            }
+        } else {
+            int P = 1;
+            while (P < u) P <<= 1;
+            for (int i = u + threadIdx.x; i < P; i += THREADS) sk[i] = std::numeric_limits<O>::max();
+            __syncthreads();
+            block_bitonic_sort<THREADS>(sk, sv, P);
+            for (int i = threadIdx.x; i < u; i += THREADS) { skey[hs + i] = sk[i]; sval[hs + i] = sv[i]; }
+        }
         __syncthreads();
         if (threadIdx.x == 0) ucnt[c] = (O)u;
         __syncthreads();

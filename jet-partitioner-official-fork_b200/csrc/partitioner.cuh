@@ -395,10 +395,10 @@ struct Engine {
             JET_CUDA(cudaFuncSetAttribute(k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
             k_contract_smem<CT_S1_THREADS, CT_S1_SLOTS, O, E, W><<<device_info().sms * 8, CT_S1_THREADS, sm1, s>>>(
-                g, map, l1.p, n1, moff.p, members.p, hrow.p, skey, sval, ucnt.p); count_launch();
+                g, map, l1.p, n1, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
             JET_LAUNCH_CHECK();
             k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W><<<device_info().sms * 2, CT_S2_THREADS, sm2, s>>>(
-                g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p); count_launch();
+                g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
             JET_LAUNCH_CHECK();
             if (dense) {
                 k_contract_dense<O, E, W><<<device_info().sms, 1024, (size_t)dense_chunk * sizeof(W), s>>>(

@@ -295,7 +295,31 @@ __device__ __forceinline__ void d_conn_warp(RefArgs<O, E, W> a, const O* list, O
         for (int s = lane; s < cap; s += 32) { keys[s] = NULL_PART; vals[s] = 0; }
         __syncwarp();
         int mine = 0;
-        mine += table_add_edges<O, E, W>(a, keys, vals, cap, rs, re, lane, 32);
+        if (cap == a.k) {
+            // direct-mapped: weights only (positive, so a nonzero sum marks
+            // a present part), keys filled in afterwards
+            for (E j0 = rs + lane; j0 < re; j0 += 4 * 32) {
+                O v[4];
+                W w[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    E j = j0 + (E)u * 32;
+                    v[u] = j < re ? a.g.adj[j] : (O)0;
+                    w[u] = j < re ? a.g.val[j] : (W)0;
+                }
+                part_t p[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) p[u] = j0 + (E)u * 32 < re ? a.part[v[u]] : NULL_PART;
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (p[u] != NULL_PART) atomic_add(&vals[p[u]], w[u]);
+            }
+            __syncwarp();
+            for (int s = lane; s < cap; s += 32)
+                if (vals[s] != 0) { keys[s] = (part_t)s; mine++; }
+        } else {
+            mine += table_add_edges<O, E, W>(a, keys, vals, cap, rs, re, lane, 32);
+        }
         __syncwarp();
         int used = group_sum<int>(mine, 32);
         smem_table_flush<W>(keys, vals, cap, used, a.k, a.slots + a.coff[i], &a.csize[i], lane, 32, false, &a.dev->err);
@@ -310,20 +334,67 @@ __global__ void __launch_bounds__(BLOCK) k_conn_warp(RefArgs<O, E, W> a, const O
 }
 
 // Any degree: one CTA per vertex, table of cap <= k slots in shared memory.
+// With `priv` (the launch gave nw * k weights of shared memory beyond the
+// table) a row with cap == k accumulates into one private direct-mapped
+// array per warp (no slot claiming, no contention between warps), which are
+// summed into the table afterwards; edge weights are positive, so a nonzero
+// sum marks a present part.
+__device__ __forceinline__ size_t conn_cta_priv_bytes(int nw, int k, size_t wbytes) {
+    return (((size_t)nw * k * wbytes + 15) & ~(size_t)15);
+}
 template <class O, class E, class W>
 __device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate,
-                                           int64_t min_deg = 0) {
+                                           int64_t min_deg = 0, int priv = 0) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_used;
     if (gate && !*gate) return;
-    part_t* keys = (part_t*)smem_raw;
-    W* vals = (W*)(smem_raw + ((a.k * sizeof(part_t) + 15) & ~(size_t)15));
+    const int nw = (int)(blockDim.x >> 5), wid = threadIdx.x >> 5;
+    W* acc = (W*)smem_raw;  // priv: nw x k
+    unsigned char* tbl = smem_raw + (priv ? conn_cta_priv_bytes(nw, a.k, sizeof(W)) : 0);
+    part_t* keys = (part_t*)tbl;
+    W* vals = (W*)(tbl + ((a.k * sizeof(part_t) + 15) & ~(size_t)15));
     for (O x = blockIdx.x; x < count; x += gridDim.x) {
         O i = list[x];
         if (only_marked && !a.mark[i]) continue;
         if ((int64_t)(a.g.row[i + 1] - a.g.row[i]) <= min_deg) continue;  // done by the warp kernel
         E rs = a.g.row[i], re = a.g.row[i + 1];
         part_t cap = conn_cap<E>(re - rs, a.k);
+        if (priv && cap == a.k) {
+            for (int s = threadIdx.x; s < nw * a.k; s += blockDim.x) acc[s] = 0;
+            if (threadIdx.x == 0) s_used = 0;
+            __syncthreads();
+            W* my = acc + wid * a.k;
+            for (E j0 = rs + threadIdx.x; j0 < re; j0 += 4 * (E)blockDim.x) {
+                O v[4];
+                W w[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    E j = j0 + (E)u * blockDim.x;
+                    v[u] = j < re ? a.g.adj[j] : (O)0;
+                    w[u] = j < re ? a.g.val[j] : (W)0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+                    if (j0 + (E)u * blockDim.x < re) atomic_add(&my[a.part[v[u]]], w[u]);
+            }
+            __syncthreads();
+            int used = 0;
+            for (int p = threadIdx.x; p < a.k; p += blockDim.x) {
+                W sum = 0;
+                for (int w = 0; w < nw; w++) sum += acc[w * a.k + p];
+                keys[p] = sum != 0 ? (part_t)p : NULL_PART;
+                vals[p] = sum;
+                used += sum != 0;
+            }
+            used = group_sum<int>(used, 32);
+            if ((threadIdx.x & 31) == 0 && used) atomicAdd(&s_used, used);
+            __syncthreads();
+            smem_table_flush<W>(keys, vals, cap, s_used, a.k, a.slots + a.coff[i], &a.csize[i], threadIdx.x, blockDim.x, true,
+                                &a.dev->err);
+            if (only_marked && threadIdx.x == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
+            __syncthreads();
+            continue;
+        }
         for (int s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = NULL_PART; vals[s] = 0; }
         if (threadIdx.x == 0) s_used = 0;
         __syncthreads();
@@ -339,8 +410,8 @@ __device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O 
 }
 template <class O, class E, class W>
 __global__ void __launch_bounds__(1024) k_conn_cta(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate,
-                                                   int64_t min_deg) {
-    d_conn_cta<O, E, W>(a, list, count, only_marked, gate, min_deg);
+                                                   int64_t min_deg, int priv) {
+    d_conn_cta<O, E, W>(a, list, count, only_marked, gate, min_deg, priv);
 }
 
 // ---------------------------------------------------------------- lookups

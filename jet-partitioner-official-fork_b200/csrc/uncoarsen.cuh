@@ -143,7 +143,7 @@ struct Refiner {
             if (k <= WARP_TABLE) {
                 k_conn_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, warp_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate, INT64_MAX); count_launch();
             } else {
-                k_conn_cta<O, E, W><<<grid_for(L.n_warp, 1) < 4096 ? grid_for(L.n_warp, 1) : 4096, 256, cta_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate, 0); count_launch();
+                k_conn_cta<O, E, W><<<grid_for(L.n_warp, 1) < 4096 ? grid_for(L.n_warp, 1) : 4096, 256, cta_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate, 0, 0); count_launch();
             }
             JET_LAUNCH_CHECK();
         }
@@ -157,7 +157,9 @@ struct Refiner {
                 cta_from = WARP_ROW_MAX;
             }
             if ((int64_t)L.max_deg > cta_from) {
-                k_conn_cta<O, E, W><<<grid_for(L.n_hub, 1) < 4096 ? grid_for(L.n_hub, 1) : 4096, 1024, cta_smem(), s>>>(a, L.hub_list.p, L.n_hub, only_marked, gate, cta_from); count_launch();
+                const int priv = k <= WARP_TABLE ? 1 : 0;
+                const size_t sm = cta_smem() + (priv ? (((size_t)32 * k * sizeof(W) + 15) & ~(size_t)15) : 0);
+                k_conn_cta<O, E, W><<<grid_for(L.n_hub, 1) < 4096 ? grid_for(L.n_hub, 1) : 4096, 1024, sm, s>>>(a, L.hub_list.p, L.n_hub, only_marked, gate, cta_from, priv); count_launch();
             }
             JET_LAUNCH_CHECK();
         }
