@@ -59,10 +59,10 @@ WORKLOADS = {
 # per-launch traffic reported is this ratio times the per-launch algorithmic
 # bytes of the timed region.
 NCU_TRAFFIC_RATIO = {
-    "conn_build": {"grid3d128": {"ratio": (126.204928 + 62.770688) / 283.246592,
-                                 "note": "ncu dram bytes of the finest-level launch (189.0 MB of 283.2 MB algorithmic), "
+    "conn_build": {"grid3d128": {"ratio": (134.903552 + 71.064320) / 283.246592,
+                                 "note": "ncu dram bytes of the finest-level launch (206.0 MB of 283.2 MB algorithmic), "
                                          "scaled to the per-launch average"}},
-    "conn_build_finest": {"grid3d128": {"ratio": (126.204928 + 62.770688) / 283.246592,
+    "conn_build_finest": {"grid3d128": {"ratio": (134.903552 + 71.064320) / 283.246592,
                                         "note": "ncu dram bytes (read + write) of the finest-level launch"}},
 }
 ALG_NAME = {0: "2-hop matching", 1: "HEC", 2: "matching"}
@@ -72,7 +72,7 @@ ITEM = {"i32": (4, 4, 4), "big": (4, 8, 8), "biggest": (8, 8, 8)}  # ordinal, of
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -89,7 +89,7 @@ class ClockSampler:
             os.close(fd)
             self.out = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.out, stderr=subprocess.DEVNULL)
+                                          "-lms", "50", "-i", str(self.gpu)], stdout=self.out, stderr=subprocess.DEVNULL)
             # wait for the first sample: nvidia-smi's start-up (NVML
             # initialisation) must not overlap the timed region
             t0 = time.time()
