@@ -275,6 +275,48 @@ __device__ __forceinline__ int table_add_edges(const RefArgs<O, E, W>& a, part_t
 
 // 32 < deg <= 4096 and k <= WARP_TABLE: one warp per vertex, table in shared memory.
 static constexpr int WARP_TABLE = 512;
+
+// One row's table built by one warp in its own shared-memory slice (`keys`,
+// `vals`: at least cap entries each).
+template <class O, class E, class W>
+__device__ __forceinline__ void conn_warp_row(const RefArgs<O, E, W>& a, O i, E rs, E re, part_t* keys, W* vals, int lane,
+                                              int only_marked) {
+    part_t cap = conn_cap<E>(re - rs, a.k);
+    for (int s = lane; s < cap; s += 32) { keys[s] = NULL_PART; vals[s] = 0; }
+    __syncwarp();
+    int mine = 0;
+    if (cap == a.k) {
+        // direct-mapped: weights only (positive, so a nonzero sum marks
+        // a present part), keys filled in afterwards
+        for (E j0 = rs + lane; j0 < re; j0 += 4 * 32) {
+            O v[4];
+            W w[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                E j = j0 + (E)u * 32;
+                v[u] = j < re ? a.g.adj[j] : (O)0;
+                w[u] = j < re ? a.g.val[j] : (W)0;
+            }
+            part_t p[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) p[u] = j0 + (E)u * 32 < re ? a.part[v[u]] : NULL_PART;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (p[u] != NULL_PART) atomic_add(&vals[p[u]], w[u]);
+        }
+        __syncwarp();
+        for (int s = lane; s < cap; s += 32)
+            if (vals[s] != 0) { keys[s] = (part_t)s; mine++; }
+    } else {
+        mine += table_add_edges<O, E, W>(a, keys, vals, cap, rs, re, lane, 32);
+    }
+    __syncwarp();
+    int used = group_sum<int>(mine, 32);
+    smem_table_flush<W>(keys, vals, cap, used, a.k, a.slots + a.coff[i], &a.csize[i], lane, 32, false, &a.dev->err);
+    if (only_marked && lane == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
+    __syncwarp();
+}
+
 template <class O, class E, class W>
 __device__ __forceinline__ void d_conn_warp(RefArgs<O, E, W> a, const O* list, O count, int only_marked, const int* gate,
                                             int64_t max_deg = INT64_MAX) {
@@ -291,40 +333,7 @@ __device__ __forceinline__ void d_conn_warp(RefArgs<O, E, W> a, const O* list, O
         if (only_marked && !a.mark[i]) continue;
         E rs = a.g.row[i], re = a.g.row[i + 1];
         if ((int64_t)(re - rs) > max_deg) continue;  // left to the CTA-per-row kernel
-        part_t cap = conn_cap<E>(re - rs, a.k);
-        for (int s = lane; s < cap; s += 32) { keys[s] = NULL_PART; vals[s] = 0; }
-        __syncwarp();
-        int mine = 0;
-        if (cap == a.k) {
-            // direct-mapped: weights only (positive, so a nonzero sum marks
-            // a present part), keys filled in afterwards
-            for (E j0 = rs + lane; j0 < re; j0 += 4 * 32) {
-                O v[4];
-                W w[4];
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    E j = j0 + (E)u * 32;
-                    v[u] = j < re ? a.g.adj[j] : (O)0;
-                    w[u] = j < re ? a.g.val[j] : (W)0;
-                }
-                part_t p[4];
-#pragma unroll
-                for (int u = 0; u < 4; u++) p[u] = j0 + (E)u * 32 < re ? a.part[v[u]] : NULL_PART;
-#pragma unroll
-                for (int u = 0; u < 4; u++)
-                    if (p[u] != NULL_PART) atomic_add(&vals[p[u]], w[u]);
-            }
-            __syncwarp();
-            for (int s = lane; s < cap; s += 32)
-                if (vals[s] != 0) { keys[s] = (part_t)s; mine++; }
-        } else {
-            mine += table_add_edges<O, E, W>(a, keys, vals, cap, rs, re, lane, 32);
-        }
-        __syncwarp();
-        int used = group_sum<int>(mine, 32);
-        smem_table_flush<W>(keys, vals, cap, used, a.k, a.slots + a.coff[i], &a.csize[i], lane, 32, false, &a.dev->err);
-        if (only_marked && lane == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
-        __syncwarp();
+        conn_warp_row<O, E, W>(a, i, rs, re, keys, vals, lane, only_marked);
     }
 }
 template <class O, class E, class W>
@@ -332,6 +341,142 @@ __global__ void __launch_bounds__(BLOCK) k_conn_warp(RefArgs<O, E, W> a, const O
                                                      int64_t max_deg) {
     d_conn_warp<O, E, W>(a, list, count, only_marked, gate, max_deg);
 }
+
+// One row with cap == k built by a whole block: every warp accumulates its
+// share of the edges into its own direct-mapped array of k weights in `acc`
+// (no slot claiming, no contention between warps); the arrays are summed into
+// the table (`keys`, `vals`: k entries each) and the table is written out.
+// Edge weights are positive, so a nonzero sum marks a present part.
+template <class O, class E, class W>
+__device__ __forceinline__ void conn_block_row_priv(const RefArgs<O, E, W>& a, O i, E rs, E re, W* acc, part_t* keys, W* vals,
+                                                    int* s_used, int only_marked) {
+    const int nw = (int)(blockDim.x >> 5), wid = threadIdx.x >> 5;
+    for (int s = threadIdx.x; s < nw * a.k; s += blockDim.x) acc[s] = 0;
+    if (threadIdx.x == 0) *s_used = 0;
+    __syncthreads();
+    W* my = acc + wid * a.k;
+    for (E j0 = rs + threadIdx.x; j0 < re; j0 += 4 * (E)blockDim.x) {
+        O v[4];
+        W w[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            E j = j0 + (E)u * blockDim.x;
+            v[u] = j < re ? a.g.adj[j] : (O)0;
+            w[u] = j < re ? a.g.val[j] : (W)0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (j0 + (E)u * blockDim.x < re) atomic_add(&my[a.part[v[u]]], w[u]);
+    }
+    __syncthreads();
+    int used = 0;
+    for (int p = threadIdx.x; p < a.k; p += blockDim.x) {
+        W sum = 0;
+        for (int w = 0; w < nw; w++) sum += acc[w * a.k + p];
+        keys[p] = sum != 0 ? (part_t)p : NULL_PART;
+        vals[p] = sum;
+        used += sum != 0;
+    }
+    used = group_sum<int>(used, 32);
+    if ((threadIdx.x & 31) == 0 && used) atomicAdd(s_used, used);
+    __syncthreads();
+    smem_table_flush<W>(keys, vals, a.k, *s_used, a.k, a.slots + a.coff[i], &a.csize[i], threadIdx.x, blockDim.x, true,
+                        &a.dev->err);
+    if (only_marked && threadIdx.x == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
+    __syncthreads();
+}
+
+// Rows of degree > THREAD_DEG (k <= WARP_TABLE), one persistent launch.
+// `order` lists them longest first (by power-of-two degree class); a shared
+// counter hands them out.  Rows of at least `block_min` edges (block_min >= k,
+// so their tables are direct-mapped) go to a whole block each, the rest to
+// single warps: a block draws rows until it draws one below block_min, gives
+// that one to its warp 0, and from then on every warp draws its own rows.
+// Longest-first keeps the long rows off the critical path's end.  The last
+// block to finish zeroes the counters for the next launch.
+//
+// Shared memory: the larger of nw * k weights + one k-entry table (block
+// rows) and nw per-warp tables of k entries (warp rows); the second is larger.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(1024, 2) k_conn_long(RefArgs<O, E, W> a, const O* order, O count, int only_marked,
+                                                   const int* gate, unsigned* ctr, int64_t block_min) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned s_x;
+    __shared__ int s_used;
+    if (gate && !*gate) return;
+    const int nw = (int)(blockDim.x >> 5), wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int k = a.k;
+    const size_t key_bytes = ((size_t)nw * k * sizeof(part_t) + 15) & ~(size_t)15;
+    bool warp_mode = false;
+    while (true) {
+        if (threadIdx.x == 0) s_x = atomicAdd(&ctr[0], 1u);
+        __syncthreads();
+        const unsigned x = s_x;
+        __syncthreads();
+        if (x >= (unsigned)count) break;
+        const O i = order[x];
+        const E rs = a.g.row[i], re = a.g.row[i + 1];
+        if ((int64_t)(re - rs) < block_min) {
+            if (wid == 0 && !(only_marked && !a.mark[i]))
+                conn_warp_row<O, E, W>(a, i, rs, re, (part_t*)smem_raw, (W*)(smem_raw + key_bytes), lane, only_marked);
+            warp_mode = true;
+            break;
+        }
+        if (only_marked && !a.mark[i]) continue;
+        W* acc = (W*)smem_raw;
+        unsigned char* tbl = smem_raw + (((size_t)nw * k * sizeof(W) + 15) & ~(size_t)15);
+        conn_block_row_priv<O, E, W>(a, i, rs, re, acc, (part_t*)tbl, (W*)(tbl + (((size_t)k * sizeof(part_t) + 15) & ~(size_t)15)),
+                                     &s_used, only_marked);
+    }
+    if (warp_mode) {
+        part_t* keys = (part_t*)smem_raw + wid * k;
+        W* vals = (W*)(smem_raw + key_bytes) + wid * k;
+        while (true) {
+            unsigned x = 0;
+            if (lane == 0) x = atomicAdd(&ctr[0], 1u);
+            x = __shfl_sync(0xffffffffu, x, 0);
+            if (x >= (unsigned)count) break;
+            const O i = order[x];
+            if (only_marked && !a.mark[i]) continue;
+            conn_warp_row<O, E, W>(a, i, a.g.row[i], a.g.row[i + 1], keys, vals, lane, only_marked);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&ctr[1], 1u) == gridDim.x - 1) {
+            ctr[0] = 0;
+            ctr[1] = 0;
+            __threadfence();
+        }
+    }
+}
+template <class W>
+__host__ __device__ constexpr size_t conn_long_smem(int nw, int k) {
+    return ((((size_t)nw * k * sizeof(part_t) + 15) & ~(size_t)15) + (size_t)nw * k * sizeof(W) + 16);
+}
+
+// Power-of-two degree class of a row of the warp or hub list, as a sort key
+// that puts longer rows first.
+template <class O, class E>
+struct GetLongKey {
+    const O* warp_list;
+    const O* hub_list;
+    O n_warp;
+    const E* row;
+    __device__ __forceinline__ uint32_t operator()(int64_t x) const {
+        O i = x < n_warp ? warp_list[x] : hub_list[x - n_warp];
+        uint64_t d = (uint64_t)(row[i + 1] - row[i]);
+        return (uint32_t)__clzll((long long)d);  // 63 - floor(log2 d), d > 0
+    }
+};
+template <class O>
+struct GetLongRow {
+    const O* warp_list;
+    const O* hub_list;
+    O n_warp;
+    __device__ __forceinline__ O operator()(int64_t x) const { return x < n_warp ? warp_list[x] : hub_list[x - n_warp]; }
+};
 
 // Any degree: one CTA per vertex, table of cap <= k slots in shared memory.
 // With `priv` (the launch gave nw * k weights of shared memory beyond the
@@ -348,7 +493,7 @@ __device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int s_used;
     if (gate && !*gate) return;
-    const int nw = (int)(blockDim.x >> 5), wid = threadIdx.x >> 5;
+    const int nw = (int)(blockDim.x >> 5);
     W* acc = (W*)smem_raw;  // priv: nw x k
     unsigned char* tbl = smem_raw + (priv ? conn_cta_priv_bytes(nw, a.k, sizeof(W)) : 0);
     part_t* keys = (part_t*)tbl;
@@ -360,39 +505,7 @@ __device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O 
         E rs = a.g.row[i], re = a.g.row[i + 1];
         part_t cap = conn_cap<E>(re - rs, a.k);
         if (priv && cap == a.k) {
-            for (int s = threadIdx.x; s < nw * a.k; s += blockDim.x) acc[s] = 0;
-            if (threadIdx.x == 0) s_used = 0;
-            __syncthreads();
-            W* my = acc + wid * a.k;
-            for (E j0 = rs + threadIdx.x; j0 < re; j0 += 4 * (E)blockDim.x) {
-                O v[4];
-                W w[4];
-#pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    E j = j0 + (E)u * blockDim.x;
-                    v[u] = j < re ? a.g.adj[j] : (O)0;
-                    w[u] = j < re ? a.g.val[j] : (W)0;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; u++)
-                    if (j0 + (E)u * blockDim.x < re) atomic_add(&my[a.part[v[u]]], w[u]);
-            }
-            __syncthreads();
-            int used = 0;
-            for (int p = threadIdx.x; p < a.k; p += blockDim.x) {
-                W sum = 0;
-                for (int w = 0; w < nw; w++) sum += acc[w * a.k + p];
-                keys[p] = sum != 0 ? (part_t)p : NULL_PART;
-                vals[p] = sum;
-                used += sum != 0;
-            }
-            used = group_sum<int>(used, 32);
-            if ((threadIdx.x & 31) == 0 && used) atomicAdd(&s_used, used);
-            __syncthreads();
-            smem_table_flush<W>(keys, vals, cap, s_used, a.k, a.slots + a.coff[i], &a.csize[i], threadIdx.x, blockDim.x, true,
-                                &a.dev->err);
-            if (only_marked && threadIdx.x == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
-            __syncthreads();
+            conn_block_row_priv<O, E, W>(a, i, rs, re, acc, keys, vals, &s_used, only_marked);
             continue;
         }
         for (int s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = NULL_PART; vals[s] = 0; }

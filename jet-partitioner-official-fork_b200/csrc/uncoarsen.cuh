@@ -39,6 +39,12 @@ struct Refiner {
     DBuf<W> cwsum;
     DBuf<uint32_t> chist;
     DBuf<O> cmarked;
+    // rows of degree > THREAD_DEG longest first (per level) and the work
+    // counters of the persistent table-build kernel
+    DBuf<O> lorder;
+    DBuf<unsigned> lctr;
+    O n_lorder = 0;
+    mutable int long_grid_cache = -1;
 
     struct HostState {
         W cut = 0;
@@ -67,6 +73,9 @@ struct Refiner {
         boff.alloc(bucket_cap, s);
         sk0.alloc(n1, s); sk1.alloc(n1, s); sv0.alloc(n1, s); sv1.alloc(n1, s); wpre.alloc(n1, s);
         redraw.alloc(n1, s); redraw_p.alloc(n1, s);
+        lorder.alloc(n1, s);
+        lctr.alloc(2, s);
+        lctr.zero();
         dev.alloc(1, s);
         dev.zero();
         ctl.alloc(1, s);
@@ -139,6 +148,13 @@ struct Refiner {
             k_conn_thread<32, 128, O, E, W><<<grid_persistent(L.n, 16), 128, 0, s>>>(a, 8, THREAD_DEG, only_marked, gate); count_launch();
         }
         JET_LAUNCH_CHECK();
+        if (k <= WARP_TABLE && n_lorder > 0) {
+            const int threads = long_threads();
+            k_conn_long<O, E, W><<<long_grid(), threads, conn_long_smem<W>(threads / 32, k), s>>>(a, lorder.p, n_lorder, only_marked, gate,
+                                                                                             lctr.p, LONG_BLOCK_MIN); count_launch();
+            JET_LAUNCH_CHECK();
+            return;
+        }
         if (L.n_warp > 0) {
             if (k <= WARP_TABLE) {
                 k_conn_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, warp_smem(), s>>>(a, L.warp_list.p, L.n_warp, only_marked, gate, INT64_MAX); count_launch();
@@ -165,6 +181,34 @@ struct Refiner {
         }
     }
     static constexpr int64_t WARP_ROW_MAX = 16384;
+    // rows of at least this many edges get a whole block in k_conn_long (a
+    // power of two >= WARP_TABLE, so whole degree classes go one way)
+    static constexpr int64_t LONG_BLOCK_MIN = 4096;
+    // levels with fewer rows of degree > THREAD_DEG keep the per-list kernels
+    static constexpr int64_t LONG_MIN_ROWS = 1024;
+    int long_threads() const { return k <= 256 ? 1024 : 512; }
+    int long_grid() const {
+        if (long_grid_cache >= 0) return long_grid_cache;
+        const void* f = (const void*)k_conn_long<O, E, W>;
+        JET_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem(f)));
+        int per_sm = 0;
+        JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, long_threads(), conn_long_smem<W>(long_threads() / 32, k)));
+        long_grid_cache = device_info().sms * (per_sm > 0 ? per_sm : 1);
+        return long_grid_cache;
+    }
+    // Orders the level's rows of degree > THREAD_DEG longest first (stable
+    // radix sort by power-of-two degree class) for k_conn_long.
+    void order_long_rows(const Level<O, E, W>& L) {
+        n_lorder = 0;
+        const int64_t cnt = (int64_t)L.n_warp + (int64_t)L.n_hub;
+        if (k > WARP_TABLE || cnt < LONG_MIN_ROWS) return;
+        GetLongKey<O, E> key{L.warp_list.p, L.hub_list.p, L.n_warp, L.row};
+        GetLongRow<O> val{L.warp_list.p, L.hub_list.p, L.n_warp};
+        // six key bits: one pass, the rows land in lorder
+        int which = radix_sort_pairs<uint32_t, O>(key, val, cnt, 6, sk0.p, lorder.p, sk1.p, sv1.p, rsort, e.scan, s);
+        if (which != 0) JET_CUDA(cudaMemcpyAsync(lorder.p, sv1.p, sizeof(O) * cnt, cudaMemcpyDeviceToDevice, s));
+        n_lorder = (O)cnt;
+    }
 
     // init_conn_data, src/jet_refiner.hpp:958-1048.  Returns sum of capacities.
     int64_t init_conn(const Level<O, E, W>& L) {
@@ -176,6 +220,7 @@ struct Refiner {
         const double bytes =
             (double)L.n * (3 * sizeof(E) + 4) + (double)L.m * (sizeof(O) + sizeof(W) + 4) + (double)C * sizeof(Slot<W>);
         const bool finest = (int64_t)L.n == (int64_t)n_max;
+        order_long_rows(L);
         int h = prof_begin(s);
         int hf = finest ? prof_begin(s) : -1;
         build_tables(L, 0, nullptr);

@@ -39,6 +39,19 @@ def make(graphs, kind, tier):
         u = torch.cat([torch.zeros(5000, dtype=torch.long), torch.arange(1, 6000)])
         v = torch.cat([torch.arange(1, 5001), torch.arange(2, 6001)])
         g = graphs.from_undirected(n, u, v, torch.randint(1, 5, (u.numel(),), generator=torch.Generator().manual_seed(1)))
+    elif kind == "dense":
+        # 1500 rows of about 100 edges, three hubs of 5000, a ring: over a
+        # thousand rows above 32 edges, so the tables go through the
+        # persistent longest-first build (whole-block and single-warp rows)
+        n = 6000
+        gen = torch.Generator().manual_seed(2)
+        u = torch.cat([torch.arange(1500).repeat_interleave(100), torch.tensor([1500, 1501, 1502]).repeat_interleave(5000),
+                       torch.arange(n)])
+        v = torch.cat([torch.randint(0, n, (150000,), generator=gen),
+                       torch.cat([torch.randperm(n, generator=gen)[:5000] for _ in range(3)]), (torch.arange(n) + 1) % n])
+        a, b = torch.minimum(u, v), torch.maximum(u, v)
+        pairs = torch.unique((a * n + b)[a != b])
+        g = graphs.from_undirected(n, pairs // n, pairs % n, torch.randint(1, 5, (pairs.numel(),), generator=gen))
     else:
         raise ValueError(kind)
     return g.as_tier(tier)
@@ -61,8 +74,8 @@ def test_contract_bit_exact(jet, graphs, orc, tier, kind):
 
 
 @pytest.mark.parametrize("tier", TIERS)
-@pytest.mark.parametrize("kind", ["grid3d", "rmat", "star"])
-@pytest.mark.parametrize("k", [8, 64, 700])
+@pytest.mark.parametrize("kind", ["grid3d", "rmat", "star", "dense"])
+@pytest.mark.parametrize("k", [8, 64, 300, 700])
 def test_conn_tables_bit_exact(jet, graphs, orc, tier, kind, k):
     g = make(graphs, kind, tier)
     og = orc.G.from_csr(g)
@@ -164,7 +177,7 @@ def test_lp_iterations_bit_exact(jet, graphs, orc, tier, kind, k):
 
 
 @pytest.mark.parametrize("tier", TIERS)
-@pytest.mark.parametrize("kind,k", [("grid2d", 8), ("grid3d", 16), ("rgg", 32), ("rmat", 16), ("star", 4)])
+@pytest.mark.parametrize("kind,k", [("grid2d", 8), ("grid3d", 16), ("rgg", 32), ("rmat", 16), ("star", 4), ("dense", 64)])
 def test_rebalance_iterations_bit_exact(jet, graphs, orc, tier, kind, k):
     """Weak and strong rebalancing reproduce the oracle's in-order bucket
     scores and destination draws: parts, sizes, cut and tables match after
@@ -192,7 +205,8 @@ def test_rebalance_iterations_bit_exact(jet, graphs, orc, tier, kind, k):
 
 @pytest.mark.parametrize("tier", TIERS)
 @pytest.mark.parametrize("kind,alg,k", [("grid2d", 1, 16), ("grid3d", 1, 32), ("rgg", 1, 8), ("rgg", 2, 16),
-                                        ("grid2d", 2, 8), ("rmat", 0, 16), ("star", 0, 8), ("rmat", 1, 32)])
+                                        ("grid2d", 2, 8), ("rmat", 0, 16), ("star", 0, 8), ("rmat", 1, 32),
+                                        ("dense", 0, 64), ("dense", 1, 300)])
 def test_full_partition_bit_exact(jet, graphs, orc, tier, kind, alg, k):
     """HEC, pure and 2-hop matching: the whole multilevel run (coarsening,
     Metis, refinement, projection) returns the oracle's partition for the
