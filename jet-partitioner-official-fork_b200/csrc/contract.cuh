@@ -48,6 +48,68 @@ __device__ __forceinline__ void block_bitonic_sort(K* key, V* val, int P) {
     }
 }
 
+// Stable LSD radix sort of u (key, value) pairs in shared memory, 8-bit
+// digits over key bits [0, bits).  Each warp owns a contiguous chunk of the
+// input; per pass it counts its digits (match.any peers, one counter per warp
+// and digit, digit-major), one block scan turns the counts into offsets, and
+// a second sweep scatters every element to its offset plus its rank among
+// equal digits before it in the chunk.  `hist` holds THREADS / 32 * 256
+// counters.  Returns the buffer that holds the result: 0 = (ka, va), 1 = (kb, vb).
+template <int THREADS, class K, class V>
+__device__ __forceinline__ int block_radix_sort_pairs(K* ka, V* va, K* kb, V* vb, int u, int bits, uint32_t* hist,
+                                                      uint32_t* s_sw) {
+    constexpr int NW = THREADS / 32;
+    constexpr int PER = NW * 256 / THREADS;  // counters per thread in the scan
+    static_assert(NW * 256 % THREADS == 0, "scan tiling");
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int chunk = (u + NW - 1) / NW;
+    const int c0 = wid * chunk < u ? wid * chunk : u;
+    const int c1 = c0 + chunk < u ? c0 + chunk : u;
+    int cur = 0;
+    for (int shift = 0; shift < bits; shift += 8) {
+        K* ks = cur == 0 ? ka : kb;
+        V* vs = cur == 0 ? va : vb;
+        K* kd = cur == 0 ? kb : ka;
+        V* vd = cur == 0 ? vb : va;
+        for (int i = threadIdx.x; i < NW * 256; i += THREADS) hist[i] = 0;
+        __syncthreads();
+        for (int b = c0; b < c1; b += 32) {
+            const int e = b + lane;
+            const bool in = e < c1;
+            const int d = in ? (int)((ks[e] >> shift) & (K)255) : 256;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            if (in && (peers & ((1u << lane) - 1u)) == 0) hist[d * NW + wid] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        uint32_t loc[PER];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int q = 0; q < PER; q++) { loc[q] = hist[threadIdx.x * PER + q]; sum += loc[q]; }
+        uint32_t tot;
+        uint32_t run = block_exclusive_scan<uint32_t>(sum, s_sw, tot);
+#pragma unroll
+        for (int q = 0; q < PER; q++) { hist[threadIdx.x * PER + q] = run; run += loc[q]; }
+        __syncthreads();
+        for (int b = c0; b < c1; b += 32) {
+            const int e = b + lane;
+            const bool in = e < c1;
+            const K key = in ? ks[e] : (K)0;
+            const int d = in ? (int)((key >> shift) & (K)255) : 256;
+            const unsigned peers = __match_any_sync(0xffffffffu, d);
+            const int rank = __popc(peers & ((1u << lane) - 1u));
+            const uint32_t base = in ? hist[d * NW + wid] : 0u;
+            if (in) { kd[base + rank] = key; vd[base + rank] = vs[e]; }
+            __syncwarp();
+            if (in && rank == 0) hist[d * NW + wid] = base + __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    return cur;
+}
+
 template <class O, class E, class W>
 __global__ void k_contract_count(GView<O, E, W> g, const O* map, O* cnt, E* du, W* cvw) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < g.n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -196,6 +258,8 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
     __shared__ int s_cnt;
     __shared__ int s_sw[32];
     O total_rows = *count;
+    int id_bits = 0;
+    while (id_bits < 63 && (((int64_t)nc - 1) >> id_bits) > 0) id_bits++;
     for (O x = blockIdx.x; x < total_rows; x += gridDim.x) {
         O c = list[x];
         E hs = hrow[c], d = hrow[c + 1] - hs;
@@ -266,6 +330,16 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
                 skey[hs + r] = key;
                 sval[hs + r] = sv[e];
             }
+        } else if (THREADS >= 512 && u > 128) {
+            // radix sort by id: the second key/value buffers and the digit
+            // counters live in the freed hash-table space
+            O* kb = (O*)ct_smem;
+            uint32_t* hist = (uint32_t*)(ct_smem + align16((size_t)(SLOTS / 2) * sizeof(O)));
+            W* vb = vals;
+            int which = block_radix_sort_pairs<THREADS, O, W>(sk, sv, kb, vb, u, id_bits, hist, (uint32_t*)s_sw);
+            const O* rk = which == 0 ? sk : kb;
+            const W* rv = which == 0 ? sv : vb;
+            for (int i = threadIdx.x; i < u; i += THREADS) { skey[hs + i] = rk[i]; sval[hs + i] = rv[i]; }
         } else {
             int P = 1;
             while (P < u) P <<= 1;

@@ -371,3 +371,32 @@ def test_contract_hub_rows_both_paths(jet, graphs, orc, tier, n):
     assert np.array_equal(host(got.adj), want.adj)
     assert np.array_equal(host(got.val), want.val)
     assert np.array_equal(host(got.vw), want.vw)
+
+
+@pytest.mark.parametrize("tier", TIERS)
+def test_contract_wide_id_range_rows(jet, graphs, orc, tier):
+    """Coarse rows of 257 to 4096 member edges whose neighbours spread over
+    more coarse ids than a shared-memory bitmap covers (about 644,000 ids): the
+    per-row radix sort path.  Rows equal the oracle's exactly."""
+    n = 1_300_000
+    gen = torch.Generator().manual_seed(9)
+    spokes = torch.arange(0, 600, 2) * 2131  # 300 vertices spread over the range
+    deg = torch.randint(300, 3000, (spokes.numel(),), generator=gen)
+    u = torch.cat([spokes.repeat_interleave(deg), torch.arange(n)])
+    v = torch.cat([torch.randint(0, n, (int(deg.sum()),), generator=gen), (torch.arange(n) + 1) % n])
+    a, b = torch.minimum(u, v), torch.maximum(u, v)
+    pairs = torch.unique((a * n + b)[a != b])
+    g = graphs.from_undirected(n, pairs // n, pairs % n, torch.randint(1, 9, (pairs.numel(),), generator=gen)).as_tier(tier)
+    og = orc.G.from_csr(g)
+    # pairs of consecutive vertices, and groups of 16 in the last 1% of ids
+    m = np.arange(n, dtype=np.int64) // 2
+    tail = n - n // 100
+    m[tail:] = tail // 2 + (np.arange(n - tail) // 16)
+    nc = int(m.max()) + 1
+    m = m.astype(np.int64 if tier == "biggest" else np.int32)
+    want = orc.contract(og, m, nc)
+    got = jet.contract(g.to("cuda"), torch.from_numpy(m).cuda(), nc)
+    assert np.array_equal(host(got.row), want.row)
+    assert np.array_equal(host(got.adj), want.adj)
+    assert np.array_equal(host(got.val), want.val)
+    assert np.array_equal(host(got.vw), want.vw)
