@@ -276,43 +276,136 @@ __device__ __forceinline__ int table_add_edges(const RefArgs<O, E, W>& a, part_t
 // 32 < deg <= 4096 and k <= WARP_TABLE: one warp per vertex, table in shared memory.
 static constexpr int WARP_TABLE = 512;
 
+// Writes a row's table from a direct-mapped accumulator: vals[p] is the
+// row's summed weight to part p (p < k; zero = absent).  A table of size k
+// stays direct-mapped; a smaller one is laid out in keys[0, size) by
+// inserting every present part from its home (shared-memory CAS, linear
+// probing), then every slot is written once, its weight read back through its
+// key.  The region holds cap = min(deg, k) slots; [size, cap) is cleared.
+// `t`/`nt` are the cooperating threads (a warp or the block; `block` picks the
+// barrier).
+template <class W>
+__device__ __forceinline__ void direct_table_write(part_t* keys, const W* vals, part_t k, part_t cap, part_t used,
+                                                   Slot<W>* base, part_t* size_out, int t, int nt, bool block, int* err) {
+    const part_t size = shrunk_size(used, cap);
+    if (size == k) {
+        for (int p = t; p < k; p += nt) {
+            Slot<W> sl;
+            sl.p = vals[p] != 0 ? (part_t)p : NULL_PART;
+            sl.v = vals[p];
+            base[p] = sl;
+        }
+    } else {
+        for (int q = t; q < size; q += nt) keys[q] = NULL_PART;
+        if (block) __syncthreads(); else __syncwarp();
+        for (int p = t; p < k; p += nt) {
+            if (vals[p] == 0) continue;
+            part_t po = slot_home((part_t)p, size, k);
+            int guard = 0;
+            while (atomicCAS((int*)&keys[po], NULL_PART, p) != NULL_PART) {
+                po = po + 1 == size ? 0 : po + 1;
+                if (++guard > size) { atomicOr(err, ERRF_OVERFLOW); break; }
+            }
+        }
+        if (block) __syncthreads(); else __syncwarp();
+        for (int q = t; q < cap; q += nt) {
+            Slot<W> sl;
+            sl.p = q < size ? keys[q] : NULL_PART;
+            sl.v = sl.p >= 0 ? vals[sl.p] : (W)0;
+            base[q] = sl;
+        }
+    }
+    if (t == 0) *size_out = size;
+}
+
+// Writes a row's table from a shared-memory hash table of cap slots (keys,
+// vals [0, cap), `used` parts present).  When the table shrinks it is
+// rehashed into keys/vals [cap, cap + size) (the caller guarantees the room)
+// and every slot of the row's region is then written once.
+template <class W>
+__device__ __forceinline__ void hashed_table_write(part_t* keys, W* vals, part_t cap, part_t used, part_t k, Slot<W>* base,
+                                                   part_t* size_out, int t, int nt, int* err) {
+    const part_t size = shrunk_size(used, cap);
+    if (size == cap) {
+        for (int q = t; q < cap; q += nt) {
+            Slot<W> sl;
+            sl.p = keys[q];
+            sl.v = vals[q];
+            base[q] = sl;
+        }
+    } else {
+        part_t* tk = keys + cap;
+        W* tv = vals + cap;
+        for (int q = t; q < size; q += nt) tk[q] = NULL_PART;
+        __syncwarp();
+        for (int q = t; q < cap; q += nt) {
+            const part_t p = keys[q];
+            if (p == NULL_PART) continue;
+            part_t po = slot_home(p, size, k);
+            int guard = 0;
+            bool placed = true;
+            while (atomicCAS((int*)&tk[po], NULL_PART, p) != NULL_PART) {
+                po = po + 1 == size ? 0 : po + 1;
+                if (++guard > size) { atomicOr(err, ERRF_OVERFLOW); placed = false; break; }
+            }
+            if (placed) tv[po] = vals[q];
+        }
+        __syncwarp();
+        for (int q = t; q < cap; q += nt) {
+            Slot<W> sl;
+            sl.p = q < size ? tk[q] : NULL_PART;
+            sl.v = sl.p >= 0 ? tv[q] : (W)0;
+            base[q] = sl;
+        }
+    }
+    if (t == 0) *size_out = size;
+}
+
 // One row's table built by one warp in its own shared-memory slice (`keys`,
-// `vals`: at least cap entries each).
+// `vals`: k entries each, k <= WARP_TABLE).  Rows with cap >= k / 4: every
+// edge adds its weight at its part's index (no hashing, no slot claiming) and
+// the table is written by direct_table_write.  Shorter rows, for which
+// clearing and scanning k entries would dominate: a hash table of cap slots,
+// rehashed in the slice's upper part when it shrinks (2 cap < k).
 template <class O, class E, class W>
 __device__ __forceinline__ void conn_warp_row(const RefArgs<O, E, W>& a, O i, E rs, E re, part_t* keys, W* vals, int lane,
                                               int only_marked) {
-    part_t cap = conn_cap<E>(re - rs, a.k);
-    for (int s = lane; s < cap; s += 32) { keys[s] = NULL_PART; vals[s] = 0; }
-    __syncwarp();
-    int mine = 0;
-    if (cap == a.k) {
-        // direct-mapped: weights only (positive, so a nonzero sum marks
-        // a present part), keys filled in afterwards
-        for (E j0 = rs + lane; j0 < re; j0 += 4 * 32) {
-            O v[4];
-            W w[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                E j = j0 + (E)u * 32;
-                v[u] = j < re ? a.g.adj[j] : (O)0;
-                w[u] = j < re ? a.g.val[j] : (W)0;
-            }
-            part_t p[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) p[u] = j0 + (E)u * 32 < re ? a.part[v[u]] : NULL_PART;
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-                if (p[u] != NULL_PART) atomic_add(&vals[p[u]], w[u]);
-        }
+    const part_t k = a.k;
+    const part_t cap = conn_cap<E>(re - rs, k);
+    if (4 * cap < k) {
+        for (int s = lane; s < cap; s += 32) { keys[s] = NULL_PART; vals[s] = 0; }
         __syncwarp();
-        for (int s = lane; s < cap; s += 32)
-            if (vals[s] != 0) { keys[s] = (part_t)s; mine++; }
-    } else {
-        mine += table_add_edges<O, E, W>(a, keys, vals, cap, rs, re, lane, 32);
+        int mine = table_add_edges<O, E, W>(a, keys, vals, cap, rs, re, lane, 32);
+        __syncwarp();
+        const int used = group_sum<int>(mine, 32);
+        hashed_table_write<W>(keys, vals, cap, used, k, a.slots + a.coff[i], &a.csize[i], lane, 32, &a.dev->err);
+        if (only_marked && lane == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
+        __syncwarp();
+        return;
+    }
+    for (int s = lane; s < k; s += 32) vals[s] = 0;
+    __syncwarp();
+    for (E j0 = rs + lane; j0 < re; j0 += 4 * 32) {
+        O v[4];
+        W w[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            E j = j0 + (E)u * 32;
+            v[u] = j < re ? a.g.adj[j] : (O)0;
+            w[u] = j < re ? a.g.val[j] : (W)0;
+        }
+        part_t p[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) p[u] = j0 + (E)u * 32 < re ? a.part[v[u]] : NULL_PART;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (p[u] != NULL_PART) atomic_add(&vals[p[u]], w[u]);
     }
     __syncwarp();
-    int used = group_sum<int>(mine, 32);
-    smem_table_flush<W>(keys, vals, cap, used, a.k, a.slots + a.coff[i], &a.csize[i], lane, 32, false, &a.dev->err);
+    int mine = 0;
+    for (int s = lane; s < k; s += 32) mine += vals[s] != 0;
+    const int used = group_sum<int>(mine, 32);
+    direct_table_write<W>(keys, vals, k, cap, used, a.slots + a.coff[i], &a.csize[i], lane, 32, false, &a.dev->err);
     if (only_marked && lane == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
     __syncwarp();
 }
@@ -373,15 +466,14 @@ __device__ __forceinline__ void conn_block_row_priv(const RefArgs<O, E, W>& a, O
     for (int p = threadIdx.x; p < a.k; p += blockDim.x) {
         W sum = 0;
         for (int w = 0; w < nw; w++) sum += acc[w * a.k + p];
-        keys[p] = sum != 0 ? (part_t)p : NULL_PART;
         vals[p] = sum;
         used += sum != 0;
     }
     used = group_sum<int>(used, 32);
     if ((threadIdx.x & 31) == 0 && used) atomicAdd(s_used, used);
     __syncthreads();
-    smem_table_flush<W>(keys, vals, a.k, *s_used, a.k, a.slots + a.coff[i], &a.csize[i], threadIdx.x, blockDim.x, true,
-                        &a.dev->err);
+    direct_table_write<W>(keys, vals, a.k, a.k, *s_used, a.slots + a.coff[i], &a.csize[i], threadIdx.x, blockDim.x, true,
+                          &a.dev->err);
     if (only_marked && threadIdx.x == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
     __syncthreads();
 }
