@@ -17,6 +17,8 @@
 namespace jetb {
 
 static constexpr int CT_S1_DU = 256, CT_S1_SLOTS = 512, CT_S1_THREADS = 128;
+static constexpr int CT_S2A_DU = 1024, CT_S2A_SLOTS = 2048, CT_S2A_THREADS = 256;
+static constexpr int CT_S2B_DU = 2048, CT_S2B_SLOTS = 4096, CT_S2B_THREADS = 512;
 static constexpr int CT_S2_DU = 4096, CT_S2_SLOTS = 8192, CT_S2_THREADS = 512;
 __host__ __device__ constexpr size_t align16(size_t b) { return (b + 15) & ~(size_t)15; }
 // hash table (slots) plus a sort buffer of slots/2 entries (a row in the bin
@@ -130,7 +132,7 @@ __global__ void k_contract_members(O n, const O* map, const O* moff, O* cnt, O* 
 }
 
 template <class O, class E>
-__global__ void k_contract_bin(O nc, const E* hrow, O* l1, O* n1, O* l2, O* n2, O* lh, O* nh) {
+__global__ void k_contract_bin(O nc, const E* hrow, O* l1, O* n1, O* l2a, O* n2a, O* l2b, O* n2b, O* l2, O* n2, O* lh, O* nh) {
     int64_t stride = (int64_t)gridDim.x * blockDim.x;
     int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int64_t rounds = ceil_div<int64_t>((int64_t)nc, stride);
@@ -140,7 +142,11 @@ __global__ void k_contract_bin(O nc, const E* hrow, O* l1, O* n1, O* l2, O* n2, 
         if (c < nc) d = hrow[c + 1] - hrow[c];
         O s = warp_append(n1, c < nc && d > 32 && d <= CT_S1_DU);
         if (s >= 0) l1[s] = (O)c;
-        s = warp_append(n2, c < nc && d > CT_S1_DU && d <= CT_S2_DU);
+        s = warp_append(n2a, c < nc && d > CT_S1_DU && d <= CT_S2A_DU);
+        if (s >= 0) l2a[s] = (O)c;
+        s = warp_append(n2b, c < nc && d > CT_S2A_DU && d <= CT_S2B_DU);
+        if (s >= 0) l2b[s] = (O)c;
+        s = warp_append(n2, c < nc && d > CT_S2B_DU && d <= CT_S2_DU);
         if (s >= 0) l2[s] = (O)c;
         s = warp_append(nh, c < nc && d > CT_S2_DU);
         if (s >= 0) lh[s] = (O)c;
@@ -257,6 +263,11 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
     __shared__ O s_mem[THREADS];
     __shared__ int s_cnt;
     __shared__ int s_sw[32];
+    // the radix sort's second buffers and counters must fit the hash table's space
+    constexpr size_t kb_bytes = align16((size_t)(SLOTS / 2) * sizeof(O));
+    constexpr size_t vb_bytes = align16((size_t)(SLOTS / 2) * sizeof(W));
+    constexpr bool radix_fits = THREADS >= 256 && kb_bytes + vb_bytes + (size_t)(THREADS / 32) * 256 * sizeof(uint32_t) <=
+                                                      align16((size_t)SLOTS * sizeof(O)) + (size_t)SLOTS * sizeof(W);
     O total_rows = *count;
     int id_bits = 0;
     while (id_bits < 63 && (((int64_t)nc - 1) >> id_bits) > 0) id_bits++;
@@ -330,13 +341,14 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
                 skey[hs + r] = key;
                 sval[hs + r] = sv[e];
             }
-        } else if (THREADS >= 512 && u > 128) {
+        } else if (radix_fits && u > 128) {
             // radix sort by id: the second key/value buffers and the digit
             // counters live in the freed hash-table space
             O* kb = (O*)ct_smem;
-            uint32_t* hist = (uint32_t*)(ct_smem + align16((size_t)(SLOTS / 2) * sizeof(O)));
-            W* vb = vals;
-            int which = block_radix_sort_pairs<THREADS, O, W>(sk, sv, kb, vb, u, id_bits, hist, (uint32_t*)s_sw);
+            W* vb = (W*)(ct_smem + kb_bytes);
+            uint32_t* hist = (uint32_t*)(ct_smem + kb_bytes + vb_bytes);
+            int which = block_radix_sort_pairs<radix_fits ? THREADS : 256, O, W>(sk, sv, kb, vb, u, id_bits, hist,
+                                                                                (uint32_t*)s_sw);
             const O* rk = which == 0 ? sk : kb;
             const W* rv = which == 0 ? sv : vb;
             for (int i = threadIdx.x; i < u; i += THREADS) { skey[hs + i] = rk[i]; sval[hs + i] = rv[i]; }
@@ -410,23 +422,56 @@ __global__ void __launch_bounds__(1024) k_contract_dense(GView<O, E, W> g, const
     }
 }
 
-// Packs each row's unique entries into the coarse CSR.
-template <class O, class E, class W>
-__global__ void __launch_bounds__(BLOCK) k_contract_copy(O nc, const E* hrow, const O* skey, const W* sval, const E* crow,
-                                                        O* cadj, W* cval) {
-#define CC_BODY(x, in, lane)                                                                \
-    {                                                                                       \
-        if (in) {                                                                           \
-            O c = (O)x;                                                                     \
-            E hs = hrow[c];                                                                 \
-            {                                                                               \
-                E o = crow[c], cnt = crow[c + 1] - o;                                       \
-                for (E t = lane; t < cnt; t += 32) { cadj[o + t] = skey[hs + t]; cval[o + t] = sval[hs + t]; } \
-            }                                                                               \
-        }                                                                                   \
+// Packs each row's unique entries into the coarse CSR as a flat copy of the
+// output in chunks of CT_COPY_CHUNK slots, one warp per chunk, so that work
+// is even whatever the row lengths.  chunk_row[j] is the row holding the
+// chunk's first slot (k_copy_chunk_rows).  The warp walks the rows from there
+// 32 at a time: lane l holds row r + l's output start, and each slot finds its
+// row by a five-step binary search over the lanes (shuffles); loads and
+// stores stay coalesced.
+static constexpr int CT_COPY_CHUNK = 2048;
+template <class O, class E>
+__global__ void k_copy_chunk_rows(O nc, const E* crow, O* chunk_row) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {
+        const E s = crow[c], t = crow[c + 1];
+        if (t <= s) continue;
+        for (E j = (s + CT_COPY_CHUNK - 1) / CT_COPY_CHUNK; j * CT_COPY_CHUNK < t; j++) chunk_row[j] = (O)c;
     }
-    JET_GROUP_LOOP(32, nc, CC_BODY)
-#undef CC_BODY
+}
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_contract_copy(O nc, E mc, const O* chunk_row, const E* hrow, const O* skey,
+                                                        const W* sval, const E* crow, O* cadj, W* cval) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+    const int64_t chunks = ((int64_t)mc + CT_COPY_CHUNK - 1) / CT_COPY_CHUNK;
+    for (int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; j < chunks; j += warps) {
+        const E e1 = (E)((j + 1) * CT_COPY_CHUNK < (int64_t)mc ? (j + 1) * CT_COPY_CHUNK : (int64_t)mc);
+        E e = (E)(j * CT_COPY_CHUNK);
+        for (int64_t r = chunk_row[j]; e < e1; r += 32) {
+            const int64_t c = r + lane;
+            const E os = c < nc ? crow[c] : mc;  // past the last row: never <= a live slot
+            const E hs = c < nc ? hrow[c] : (E)0;
+            const E wend = r + 32 < (int64_t)nc ? crow[r + 32] : mc;
+            const E lim = wend < e1 ? wend : e1;
+            for (E base = e; base < lim; base += 32) {
+                const E x = base + lane;
+                int lo = 0;
+#pragma unroll
+                for (int step = 16; step > 0; step >>= 1) {
+                    const E v = __shfl_sync(0xffffffffu, os, lo + step);
+                    if (v <= x) lo += step;
+                }
+                const E ro = __shfl_sync(0xffffffffu, os, lo);
+                const E rh = __shfl_sync(0xffffffffu, hs, lo);
+                if (x < lim) {
+                    const E src = rh + (x - ro);
+                    cadj[x] = skey[src];
+                    cval[x] = sval[src];
+                }
+            }
+            e = lim;
+        }
+    }
 }
 
 // ---------------------------------------------------------------- hub rows, many coarse ids

@@ -372,11 +372,13 @@ struct Engine {
         W* sval;
         if (skey_buf && skey_buf->n >= (int64_t)L.m) { skey = skey_buf->p; sval = sval_buf->p; }
         else { skey_own.alloc(L.m > 0 ? L.m : 1, s); sval_own.alloc(L.m > 0 ? L.m : 1, s); skey = skey_own.p; sval = sval_own.p; }
-        DBuf<O> l1(nc, s), l2(nc, s), lh(nc, s);
+        DBuf<O> l1(nc, s), l2a(nc, s), l2b(nc, s), l2(nc, s), lh(nc, s);
         O* n1 = dslot<O>(40);
         O* n2 = dslot<O>(41);
         O* nh = dslot<O>(42);
         int* err = dslot<int>(43);
+        O* n2a = dslot<O>(45);
+        O* n2b = dslot<O>(47);
         // hub rows: a dense shared-memory accumulator when the coarse id range
         // takes at most DENSE_PASSES chunks, else (row, neighbour) keys + radix sort
         int dense_chunk = (max_dynamic_smem((const void*)k_contract_dense<O, E, W>) - 1024) / (int)sizeof(W);
@@ -385,17 +387,34 @@ struct Engine {
         if (dense)
             JET_CUDA(cudaFuncSetAttribute(k_contract_dense<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           max_dynamic_smem((const void*)k_contract_dense<O, E, W>)));
-        JET_CUDA(cudaMemsetAsync(n1, 0, 4 * sizeof(int64_t), s));
-        k_contract_bin<O, E><<<grid_persistent(nc, 8), BLOCK, 0, s>>>(nc, hrow.p, l1.p, n1, l2.p, n2, lh.p, nh); count_launch();
+        JET_CUDA(cudaMemsetAsync(n1, 0, 8 * sizeof(int64_t), s));  // slots 40-47 (44 and 46 are scan totals, set later)
+        k_contract_bin<O, E><<<grid_persistent(nc, 8), BLOCK, 0, s>>>(nc, hrow.p, l1.p, n1, l2a.p, n2a, l2b.p, n2b, l2.p, n2, lh.p, nh);
+        count_launch();
         JET_LAUNCH_CHECK();
         k_contract_warp<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(g, map, nc, moff.p, members.p, hrow.p, skey, sval, ucnt.p); count_launch();
         JET_LAUNCH_CHECK();
         {
-            size_t sm1 = contract_smem_bytes<O, W>(CT_S1_SLOTS), sm2 = contract_smem_bytes<O, W>(CT_S2_SLOTS);
+            size_t sm1 = contract_smem_bytes<O, W>(CT_S1_SLOTS), sm2a = contract_smem_bytes<O, W>(CT_S2A_SLOTS),
+                   sm2b = contract_smem_bytes<O, W>(CT_S2B_SLOTS), sm2 = contract_smem_bytes<O, W>(CT_S2_SLOTS);
+            JET_CUDA(cudaFuncSetAttribute(k_contract_smem<CT_S2B_THREADS, CT_S2B_SLOTS, O, E, W>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2b));
             JET_CUDA(cudaFuncSetAttribute(k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+            JET_CUDA(cudaFuncSetAttribute(k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2a));
             k_contract_smem<CT_S1_THREADS, CT_S1_SLOTS, O, E, W><<<device_info().sms * 8, CT_S1_THREADS, sm1, s>>>(
                 g, map, l1.p, n1, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
+            JET_LAUNCH_CHECK();
+            int per_sm = 0;
+            JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W>,
+                                                                   CT_S2A_THREADS, sm2a));
+            k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W><<<device_info().sms * (per_sm > 0 ? per_sm : 1), CT_S2A_THREADS, sm2a, s>>>(
+                g, map, l2a.p, n2a, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
+            JET_LAUNCH_CHECK();
+            JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contract_smem<CT_S2B_THREADS, CT_S2B_SLOTS, O, E, W>,
+                                                                   CT_S2B_THREADS, sm2b));
+            k_contract_smem<CT_S2B_THREADS, CT_S2B_SLOTS, O, E, W><<<device_info().sms * (per_sm > 0 ? per_sm : 1), CT_S2B_THREADS, sm2b, s>>>(
+                g, map, l2b.p, n2b, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
             JET_LAUNCH_CHECK();
             k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W><<<device_info().sms * 2, CT_S2_THREADS, sm2, s>>>(
                 g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
@@ -421,9 +440,15 @@ struct Engine {
         C.own_adj.alloc(mc > 0 ? mc : 1, s);
         C.own_val.alloc(mc > 0 ? mc : 1, s);
         // every row's unique entries are packed at its scratch offset, in neighbour order
-        k_contract_copy<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(nc, hrow.p, skey, sval, C.own_row.p,
-                                                                                        C.own_adj.p, C.own_val.p); count_launch();
-        JET_LAUNCH_CHECK();
+        if (mc > 0) {
+            const int64_t chunks = ((int64_t)mc + CT_COPY_CHUNK - 1) / CT_COPY_CHUNK;
+            DBuf<O> chunk_row(chunks, s);
+            k_copy_chunk_rows<O, E><<<grid_persistent(nc, 8), BLOCK, 0, s>>>(nc, C.own_row.p, chunk_row.p); count_launch();
+            k_contract_copy<O, E, W><<<grid_persistent(chunks * 32, 16), BLOCK, 0, s>>>(nc, mc, chunk_row.p, hrow.p, skey, sval,
+                                                                                      C.own_row.p, C.own_adj.p, C.own_val.p);
+            count_launch();
+            JET_LAUNCH_CHECK();
+        }
         C.row = C.own_row.p;
         C.adj = C.own_adj.p;
         C.val = C.own_val.p;
