@@ -516,13 +516,17 @@ __global__ void __launch_bounds__(BLOCK) k_twin_hash(GView<O, E, W> g, const O* 
     JET_GROUP_LOOP(32, cnt, TWIN_BODY)
 #undef TWIN_BODY
 }
+// Hub rows (deg > HUB_DEG) of the unmatched list, one CTA each: walks the
+// level's hub list and writes each unmatched hub's digest at its list
+// position pos[u].
 template <class O, class E, class W>
-__global__ void __launch_bounds__(1024) k_twin_hash_hub(GView<O, E, W> g, const O* list, O cnt, uint64_t* hashes) {
+__global__ void __launch_bounds__(1024) k_twin_hash_hub(GView<O, E, W> g, const O* hub_list, O n_hub, const O* vcmap,
+                                                        const O* pos, uint64_t* hashes) {
     __shared__ uint64_t part[32];
-    for (O x = blockIdx.x; x < cnt; x += gridDim.x) {
-        O u = list[x];
+    for (O x = blockIdx.x; x < n_hub; x += gridDim.x) {
+        O u = hub_list[x];
+        if (vcmap[u] != ord_max<O>()) continue;
         E s = g.row[u], e = g.row[u + 1];
-        if (e - s <= HUB_DEG) continue;
         uint64_t h = 0;
         for (E j = s + threadIdx.x; j < e; j += blockDim.x) { uint64_t y = pod_hash(g.adj[j]); h += y * y + y; }
         h = group_sum<uint64_t>(h, 32);
@@ -530,7 +534,7 @@ __global__ void __launch_bounds__(1024) k_twin_hash_hub(GView<O, E, W> g, const 
         __syncthreads();
         if (threadIdx.x == 0) {
             for (int w = 1; w < (int)(blockDim.x >> 5); w++) h += part[w];
-            hashes[x] = h;
+            hashes[pos[u]] = h;
         }
         __syncthreads();
     }

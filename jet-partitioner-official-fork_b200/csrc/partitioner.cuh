@@ -228,9 +228,13 @@ struct Engine {
         return *(O*)hscal;
     }
 
-    O unmatched_list(Level<O, E, W>& L, const O* vcmap, int leaves_only, DBuf<O>& list) {
+    // Unmatched vertices (leaves only: of degree 1) in vertex order; pos_out,
+    // if given, receives each vertex's position in the list.
+    O unmatched_list(Level<O, E, W>& L, const O* vcmap, int leaves_only, DBuf<O>& list, DBuf<O>* pos_out = nullptr) {
         O n = L.n;
-        DBuf<O> pos(n, s);
+        DBuf<O> pos_own;
+        DBuf<O>& pos = pos_out ? *pos_out : pos_own;
+        pos.alloc(n > 0 ? n : 1, s);
         O* total = dslot<O>(25);
         exclusive_scan<O, GetUnmatched<O, E>>(GetUnmatched<O, E>{vcmap, L.row, leaves_only}, n, pos.p, total, scan, s);
         JET_CUDA(cudaMemcpyAsync(hscal, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -281,13 +285,15 @@ struct Engine {
         unmapped = count_unmatched(n, vcmap);
         if ((double)unmapped / (double)n > 0.25) {  // twins, src/heuristics.hpp:565-598
             DBuf<O> list;
-            O cnt = unmatched_list(L, vcmap, 0, list);
+            DBuf<O> pos;
+            O cnt = unmatched_list(L, vcmap, 0, list, &pos);
             if (cnt > 0) {
                 DBuf<uint64_t> hs(cnt, s);
                 k_twin_hash<O, E, W><<<grid_persistent((int64_t)cnt * 32, 16), BLOCK, 0, s>>>(g, list.p, cnt, hs.p); count_launch();
                 JET_LAUNCH_CHECK();
                 if (L.n_hub > 0) {
-                    k_twin_hash_hub<O, E, W><<<grid_for(cnt, 1) < 4096 ? grid_for(cnt, 1) : 4096, 1024, 0, s>>>(g, list.p, cnt, hs.p); count_launch();
+                    k_twin_hash_hub<O, E, W><<<grid_for(L.n_hub, 1) < 4096 ? grid_for(L.n_hub, 1) : 4096, 1024, 0, s>>>(
+                        g, L.hub_list.p, L.n_hub, vcmap, pos.p, hs.p); count_launch();
                     JET_LAUNCH_CHECK();
                 }
                 match_hash<uint64_t>(list.p, hs.p, cnt, (uint64_t)0, (uint64_t)0, 64, vcmap);

@@ -443,10 +443,10 @@ __global__ void __launch_bounds__(BLOCK) k_conn_warp(RefArgs<O, E, W> a, const O
 template <class O, class E, class W>
 __device__ __forceinline__ void conn_block_row_priv(const RefArgs<O, E, W>& a, O i, E rs, E re, W* acc, part_t* keys, W* vals,
                                                     int* s_used, int only_marked) {
+    // acc is all zero on entry (conn_priv_zero before the first row) and is
+    // left all zero: the merge clears every entry it reads
     const int nw = (int)(blockDim.x >> 5), wid = threadIdx.x >> 5;
-    for (int s = threadIdx.x; s < nw * a.k; s += blockDim.x) acc[s] = 0;
     if (threadIdx.x == 0) *s_used = 0;
-    __syncthreads();
     W* my = acc + wid * a.k;
     for (E j0 = rs + threadIdx.x; j0 < re; j0 += 4 * (E)blockDim.x) {
         O v[4];
@@ -462,10 +462,12 @@ __device__ __forceinline__ void conn_block_row_priv(const RefArgs<O, E, W>& a, O
             if (j0 + (E)u * blockDim.x < re) atomic_add(&my[a.part[v[u]]], w[u]);
     }
     __syncthreads();
+    // merge: one thread per part sums the nw arrays (consecutive parts on
+    // consecutive lanes: no bank conflicts), clearing each entry it reads
     int used = 0;
     for (int p = threadIdx.x; p < a.k; p += blockDim.x) {
         W sum = 0;
-        for (int w = 0; w < nw; w++) sum += acc[w * a.k + p];
+        for (int w = 0; w < nw; w++) { sum += acc[w * a.k + p]; acc[w * a.k + p] = 0; }
         vals[p] = sum;
         used += sum != 0;
     }
@@ -475,6 +477,13 @@ __device__ __forceinline__ void conn_block_row_priv(const RefArgs<O, E, W>& a, O
     direct_table_write<W>(keys, vals, a.k, a.k, *s_used, a.slots + a.coff[i], &a.csize[i], threadIdx.x, blockDim.x, true,
                           &a.dev->err);
     if (only_marked && threadIdx.x == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
+    __syncthreads();
+}
+
+// Clears the per-warp accumulators of conn_block_row_priv once per block.
+template <class W>
+__device__ __forceinline__ void conn_priv_zero(W* acc, int entries) {
+    for (int s = threadIdx.x; s < entries; s += blockDim.x) acc[s] = 0;
     __syncthreads();
 }
 
@@ -500,6 +509,9 @@ __global__ void __launch_bounds__(1024, 2) k_conn_long(RefArgs<O, E, W> a, const
     const int k = a.k;
     const size_t key_bytes = ((size_t)nw * k * sizeof(part_t) + 15) & ~(size_t)15;
     bool warp_mode = false;
+    O pending = 0;  // warp 0: the first warp row, drawn by the whole block
+    bool has_pending = false;
+    conn_priv_zero<W>((W*)smem_raw, nw * k);
     while (true) {
         if (threadIdx.x == 0) s_x = atomicAdd(&ctr[0], 1u);
         __syncthreads();
@@ -509,8 +521,7 @@ __global__ void __launch_bounds__(1024, 2) k_conn_long(RefArgs<O, E, W> a, const
         const O i = order[x];
         const E rs = a.g.row[i], re = a.g.row[i + 1];
         if ((int64_t)(re - rs) < block_min) {
-            if (wid == 0 && !(only_marked && !a.mark[i]))
-                conn_warp_row<O, E, W>(a, i, rs, re, (part_t*)smem_raw, (W*)(smem_raw + key_bytes), lane, only_marked);
+            if (wid == 0) { pending = i; has_pending = true; }
             warp_mode = true;
             break;
         }
@@ -524,11 +535,17 @@ __global__ void __launch_bounds__(1024, 2) k_conn_long(RefArgs<O, E, W> a, const
         part_t* keys = (part_t*)smem_raw + wid * k;
         W* vals = (W*)(smem_raw + key_bytes) + wid * k;
         while (true) {
-            unsigned x = 0;
-            if (lane == 0) x = atomicAdd(&ctr[0], 1u);
-            x = __shfl_sync(0xffffffffu, x, 0);
-            if (x >= (unsigned)count) break;
-            const O i = order[x];
+            O i;
+            if (has_pending) {
+                i = pending;
+                has_pending = false;
+            } else {
+                unsigned x = 0;
+                if (lane == 0) x = atomicAdd(&ctr[0], 1u);
+                x = __shfl_sync(0xffffffffu, x, 0);
+                if (x >= (unsigned)count) break;
+                i = order[x];
+            }
             if (only_marked && !a.mark[i]) continue;
             conn_warp_row<O, E, W>(a, i, a.g.row[i], a.g.row[i + 1], keys, vals, lane, only_marked);
         }
@@ -590,6 +607,7 @@ __device__ __forceinline__ void d_conn_cta(RefArgs<O, E, W> a, const O* list, O 
     unsigned char* tbl = smem_raw + (priv ? conn_cta_priv_bytes(nw, a.k, sizeof(W)) : 0);
     part_t* keys = (part_t*)tbl;
     W* vals = (W*)(tbl + ((a.k * sizeof(part_t) + 15) & ~(size_t)15));
+    if (priv) conn_priv_zero<W>(acc, nw * a.k);
     for (O x = blockIdx.x; x < count; x += gridDim.x) {
         O i = list[x];
         if (only_marked && !a.mark[i]) continue;

@@ -186,7 +186,9 @@ struct Refiner {
     static constexpr int64_t LONG_BLOCK_MIN = 4096;
     // levels with fewer rows of degree > THREAD_DEG keep the per-list kernels
     static constexpr int64_t LONG_MIN_ROWS = 1024;
-    int long_threads() const { return k <= 256 ? 1024 : 512; }
+    // 1024 threads, two blocks per SM (measured against 512 x 4: faster on
+    // levels dominated by single-warp rows, even on whole-block rows)
+    int long_threads() const { return 1024; }
     int long_grid() const {
         if (long_grid_cache >= 0) return long_grid_cache;
         const void* f = (const void*)k_conn_long<O, E, W>;
