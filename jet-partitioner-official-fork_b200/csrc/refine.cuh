@@ -99,9 +99,10 @@ struct RefArgs {
 // Rows with dlo < deg <= dhi (dhi <= SET <= 32): one thread per vertex, its
 // distinct parts gathered in a private SET-entry shared-memory set
 // (interleaved so threads hit distinct banks; multiplicative hash into a
-// power-of-two set, no division).  Two instances cover deg <= 32: SET = 8
-// (256 threads, small enough for full occupancy) for deg <= 8 and SET = 32
-// for 8 < deg <= 32, launched only when the level has such rows.
+// power-of-two set, no division).  Three instances cover deg <= 32: SET = 8
+// (256 threads, small enough for full occupancy) for deg <= 8, SET = 16 (256
+// threads) for 8 < deg <= 16 and SET = 32 (128 threads) for 16 < deg <= 32,
+// the last two launched only when the level has such rows.
 // Neighbours are read in batches of 8 with every load issued before the first
 // use, so a row costs about two memory latencies instead of two per entry.
 // The final table (at most 32 slots) is laid out with a register bitmask of
@@ -112,14 +113,19 @@ __device__ __forceinline__ int set_home(part_t p) {
     return (int)(((uint32_t)p * 0x9E3779B1u) >> (32 - bits));
 }
 
+// With a list (rows of one degree class, *list_count of them, from
+// k_bin_short) the threads walk the list instead of every vertex, so whole
+// warps stay busy.
 template <int SET, int THREADS, class O, class E, class W>
-__global__ void __launch_bounds__(THREADS) k_conn_thread(RefArgs<O, E, W> a, int dlo, int dhi, int only_marked, const int* gate) {
+__global__ void __launch_bounds__(THREADS) k_conn_thread(RefArgs<O, E, W> a, int dlo, int dhi, int only_marked, const int* gate,
+                                                        const O* list, const O* list_count) {
     __shared__ part_t sk[SET][THREADS];
     __shared__ W sv[SET][THREADS];
     if (gate && !*gate) return;
     const int t = threadIdx.x;
-    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + t; x < a.g.n; x += (int64_t)gridDim.x * blockDim.x) {
-        O i = (O)x;
+    const int64_t count = list ? (int64_t)*list_count : (int64_t)a.g.n;
+    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + t; x < count; x += (int64_t)gridDim.x * blockDim.x) {
+        O i = list ? list[x] : (O)x;
         E rs = a.g.row[i], re = a.g.row[i + 1];
         E deg = re - rs;
         if (deg <= dlo || deg > dhi) continue;
@@ -182,6 +188,24 @@ __global__ void __launch_bounds__(THREADS) k_conn_thread(RefArgs<O, E, W> a, int
         if (!ok) atomicOr(&a.dev->err, ERRF_OVERFLOW);
         a.csize[i] = size;
         if (only_marked) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
+    }
+}
+
+// Rows of 9-16 and of 17-32 edges into two lists (counts in cnt[0], cnt[1])
+// for the SET = 16 and SET = 32 table builds.
+template <class O, class E>
+__global__ void k_bin_short(O n, const E* row, O* l16, O* l32, O* cnt) {
+    int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    int64_t rounds = ceil_div<int64_t>((int64_t)n, stride);
+    for (int64_t r = 0; r < rounds; r++) {
+        int64_t i = start + r * stride;
+        E d = 0;
+        if (i < n) d = row[i + 1] - row[i];
+        O s = warp_append(&cnt[0], i < n && d > 8 && d <= 16);
+        if (s >= 0) l16[s] = (O)i;
+        s = warp_append(&cnt[1], i < n && d > 16 && d <= THREAD_DEG);
+        if (s >= 0) l32[s] = (O)i;
     }
 }
 

@@ -43,6 +43,8 @@ struct Refiner {
     // counters of the persistent table-build kernel
     DBuf<O> lorder;
     DBuf<unsigned> lctr;
+    // rows of 9-16 and of 17-32 edges (per level) and their counts
+    DBuf<O> s16, s32, scnt;
     O n_lorder = 0;
     mutable int long_grid_cache = -1;
 
@@ -74,6 +76,9 @@ struct Refiner {
         sk0.alloc(n1, s); sk1.alloc(n1, s); sv0.alloc(n1, s); sv1.alloc(n1, s); wpre.alloc(n1, s);
         redraw.alloc(n1, s); redraw_p.alloc(n1, s);
         lorder.alloc(n1, s);
+        s16.alloc(n1, s);
+        s32.alloc(n1, s);
+        scnt.alloc(2, s);
         lctr.alloc(2, s);
         lctr.zero();
         dev.alloc(1, s);
@@ -143,9 +148,13 @@ struct Refiner {
         auto a = args(L);
         if (cta_smem() > (size_t)device_info().max_smem_optin - 1024)
             throw JetError{JET_ERR_INVALID, "num_parts too large for the shared-memory connectivity tables"};
-        k_conn_thread<8, 256, O, E, W><<<grid_persistent(L.n, 8), 256, 0, s>>>(a, -1, 8, only_marked, gate); count_launch();
+        k_conn_thread<8, 256, O, E, W><<<grid_persistent(L.n, 8), 256, 0, s>>>(a, -1, 8, only_marked, gate, nullptr, nullptr); count_launch();
         if (L.max_deg > 8) {
-            k_conn_thread<32, 128, O, E, W><<<grid_persistent(L.n, 16), 128, 0, s>>>(a, 8, THREAD_DEG, only_marked, gate); count_launch();
+            k_conn_thread<16, 256, O, E, W><<<grid_persistent(L.n, 8), 256, 0, s>>>(a, 8, 16, only_marked, gate, s16.p, scnt.p); count_launch();
+        }
+        if (L.max_deg > 16) {
+            k_conn_thread<32, 128, O, E, W><<<grid_persistent(L.n, 16), 128, 0, s>>>(a, 16, THREAD_DEG, only_marked, gate, s32.p,
+                                                                                  scnt.p + 1); count_launch();
         }
         JET_LAUNCH_CHECK();
         if (k <= WARP_TABLE && n_lorder > 0) {
@@ -198,10 +207,16 @@ struct Refiner {
         long_grid_cache = device_info().sms * (per_sm > 0 ? per_sm : 1);
         return long_grid_cache;
     }
-    // Orders the level's rows of degree > THREAD_DEG longest first (stable
-    // radix sort by power-of-two degree class) for k_conn_long.
+    // Per-level row lists for the table builds: rows of 9-16 and of 17-32
+    // edges (k_bin_short), and rows of degree > THREAD_DEG longest first
+    // (stable radix sort by power-of-two degree class) for k_conn_long.
     void order_long_rows(const Level<O, E, W>& L) {
         n_lorder = 0;
+        if (L.max_deg > 8) {
+            JET_CUDA(cudaMemsetAsync(scnt.p, 0, 2 * sizeof(O), s));
+            k_bin_short<O, E><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(L.n, L.row, s16.p, s32.p, scnt.p); count_launch();
+            JET_LAUNCH_CHECK();
+        }
         const int64_t cnt = (int64_t)L.n_warp + (int64_t)L.n_hub;
         if (k > WARP_TABLE || cnt < LONG_MIN_ROWS) return;
         GetLongKey<O, E> key{L.warp_list.p, L.hub_list.p, L.n_warp, L.row};
