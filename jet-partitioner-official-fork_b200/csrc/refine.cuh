@@ -93,7 +93,19 @@ struct RefArgs {
     O* moves_hub;
     RefDev<O, W>* dev;
     const double* filter;  // LP filter ratio, read on the device (it changes per iteration with ultra settings)
+    int narrow;            // every row's summed edge weight fits in 32 bits (see acc_add)
 };
+
+// Adds w to a shared-memory accumulator.  With 64-bit weights and `narrow`
+// (the level's total edge weight is below 2^31, so no partial sum of a row
+// reaches 2^32) the add is a 32-bit atomic on the low word: the high word
+// stays zero and the 64-bit value is exact.  A 64-bit shared atomic add
+// costs several times as much.
+template <class W>
+__device__ __forceinline__ void acc_add(W* p, W w, int narrow) {
+    if (sizeof(W) == 8 && narrow) atomicAdd((unsigned*)p, (unsigned)w);
+    else atomic_add(p, w);
+}
 
 // ---------------------------------------------------------------- table build
 // Rows with dlo < deg <= dhi (dhi <= SET <= 32): one thread per vertex, its
@@ -214,7 +226,8 @@ __global__ void k_bin_short(O n, const E* row, O* l16, O* l32, O* cnt) {
 // `err` receives ERRF_OVERFLOW if the probe sequence exceeds its bound (the
 // table always has room: cap >= number of distinct neighbour parts).
 template <class W>
-__device__ __forceinline__ bool smem_table_add(part_t* keys, W* vals, part_t cap, part_t k, part_t p, W w, int* err) {
+__device__ __forceinline__ bool smem_table_add(part_t* keys, W* vals, part_t cap, part_t k, part_t p, W w, int* err,
+                                               int narrow = 0) {
     volatile part_t* vk = keys;
     part_t po = slot_home(p, cap, k);
     bool claimed = false;
@@ -237,7 +250,7 @@ __device__ __forceinline__ bool smem_table_add(part_t* keys, W* vals, part_t cap
             if (++guard > 2 * cap) { atomicOr(err, ERRF_OVERFLOW); return false; }
         }
     }
-    atomic_add(&vals[po], w);
+    acc_add<W>(&vals[po], w, narrow);
     return claimed;
 }
 
@@ -292,7 +305,7 @@ __device__ __forceinline__ int table_add_edges(const RefArgs<O, E, W>& a, part_t
         for (int u = 0; u < 4; u++) p[u] = j0 + (E)u * nt < re ? a.part[v[u]] : NULL_PART;
 #pragma unroll
         for (int u = 0; u < 4; u++)
-            if (p[u] != NULL_PART) mine += smem_table_add<W>(keys, vals, cap, a.k, p[u], w[u], &a.dev->err);
+            if (p[u] != NULL_PART) mine += smem_table_add<W>(keys, vals, cap, a.k, p[u], w[u], &a.dev->err, a.narrow);
     }
     return mine;
 }
@@ -308,16 +321,18 @@ static constexpr int WARP_TABLE = 512;
 // key.  The region holds cap = min(deg, k) slots; [size, cap) is cleared.
 // `t`/`nt` are the cooperating threads (a warp or the block; `block` picks the
 // barrier).
+// With `clear`, every weight read is zeroed, leaving vals all zero.
 template <class W>
-__device__ __forceinline__ void direct_table_write(part_t* keys, const W* vals, part_t k, part_t cap, part_t used,
-                                                   Slot<W>* base, part_t* size_out, int t, int nt, bool block, int* err) {
+__device__ __forceinline__ void direct_table_write(part_t* keys, W* vals, part_t k, part_t cap, part_t used, Slot<W>* base,
+                                                   part_t* size_out, int t, int nt, bool block, int* err, bool clear = false) {
     const part_t size = shrunk_size(used, cap);
     if (size == k) {
         for (int p = t; p < k; p += nt) {
             Slot<W> sl;
-            sl.p = vals[p] != 0 ? (part_t)p : NULL_PART;
             sl.v = vals[p];
+            sl.p = sl.v != 0 ? (part_t)p : NULL_PART;
             base[p] = sl;
+            if (clear && sl.v != 0) vals[p] = 0;
         }
     } else {
         for (int q = t; q < size; q += nt) keys[q] = NULL_PART;
@@ -337,6 +352,7 @@ __device__ __forceinline__ void direct_table_write(part_t* keys, const W* vals, 
             sl.p = q < size ? keys[q] : NULL_PART;
             sl.v = sl.p >= 0 ? vals[sl.p] : (W)0;
             base[q] = sl;
+            if (clear && sl.p >= 0) vals[sl.p] = 0;  // each present part sits in one slot
         }
     }
     if (t == 0) *size_out = size;
@@ -356,6 +372,7 @@ __device__ __forceinline__ void hashed_table_write(part_t* keys, W* vals, part_t
             sl.p = keys[q];
             sl.v = vals[q];
             base[q] = sl;
+            vals[q] = 0;
         }
     } else {
         part_t* tk = keys + cap;
@@ -380,17 +397,21 @@ __device__ __forceinline__ void hashed_table_write(part_t* keys, W* vals, part_t
             sl.p = q < size ? tk[q] : NULL_PART;
             sl.v = sl.p >= 0 ? tv[q] : (W)0;
             base[q] = sl;
+            vals[q] = 0;
+            if (q < size) tv[q] = 0;
         }
     }
     if (t == 0) *size_out = size;
 }
 
 // One row's table built by one warp in its own shared-memory slice (`keys`,
-// `vals`: k entries each, k <= WARP_TABLE).  Rows with cap >= k / 4: every
-// edge adds its weight at its part's index (no hashing, no slot claiming) and
-// the table is written by direct_table_write.  Shorter rows, for which
-// clearing and scanning k entries would dominate: a hash table of cap slots,
-// rehashed in the slice's upper part when it shrinks (2 cap < k).
+// `vals`: k entries each, k <= WARP_TABLE; vals all zero on entry, and left
+// all zero).  Rows with cap >= k / 4: every edge adds its weight at its
+// part's index (no hashing, no slot claiming), the nonzero entries are
+// counted, and the table is written by direct_table_write, which clears what
+// it reads (no clearing pass per row).  Shorter rows, for which scanning k entries would
+// dominate: a hash table of cap slots, rehashed in the slice's upper part
+// when it shrinks (2 cap < k).
 template <class O, class E, class W>
 __device__ __forceinline__ void conn_warp_row(const RefArgs<O, E, W>& a, O i, E rs, E re, part_t* keys, W* vals, int lane,
                                               int only_marked) {
@@ -407,8 +428,6 @@ __device__ __forceinline__ void conn_warp_row(const RefArgs<O, E, W>& a, O i, E 
         __syncwarp();
         return;
     }
-    for (int s = lane; s < k; s += 32) vals[s] = 0;
-    __syncwarp();
     for (E j0 = rs + lane; j0 < re; j0 += 4 * 32) {
         O v[4];
         W w[4];
@@ -423,13 +442,13 @@ __device__ __forceinline__ void conn_warp_row(const RefArgs<O, E, W>& a, O i, E 
         for (int u = 0; u < 4; u++) p[u] = j0 + (E)u * 32 < re ? a.part[v[u]] : NULL_PART;
 #pragma unroll
         for (int u = 0; u < 4; u++)
-            if (p[u] != NULL_PART) atomic_add(&vals[p[u]], w[u]);
+            if (p[u] != NULL_PART) acc_add<W>(&vals[p[u]], w[u], a.narrow);
     }
     __syncwarp();
     int mine = 0;
     for (int s = lane; s < k; s += 32) mine += vals[s] != 0;
     const int used = group_sum<int>(mine, 32);
-    direct_table_write<W>(keys, vals, k, cap, used, a.slots + a.coff[i], &a.csize[i], lane, 32, false, &a.dev->err);
+    direct_table_write<W>(keys, vals, k, cap, used, a.slots + a.coff[i], &a.csize[i], lane, 32, false, &a.dev->err, true);
     if (only_marked && lane == 0) { a.mark[i] = 0; a.dest_cache[i] = NULL_PART; }
     __syncwarp();
 }
@@ -444,6 +463,8 @@ __device__ __forceinline__ void d_conn_warp(RefArgs<O, E, W> a, const O* list, O
     const int nw = (int)(blockDim.x >> 5);
     part_t* keys = (part_t*)smem_raw + wid * kw;
     W* vals = (W*)(smem_raw + (((size_t)nw * kw * sizeof(part_t) + 15) & ~(size_t)15)) + wid * kw;
+    for (int s = lane; s < kw; s += 32) vals[s] = 0;  // conn_warp_row keeps it zero
+    __syncwarp();
     const int64_t warps = (int64_t)gridDim.x * nw;
     for (int64_t x = blockIdx.x * (int64_t)nw + wid; x < count; x += warps) {
         O i = list ? list[x] : (O)x;  // no list: every vertex
@@ -483,7 +504,7 @@ __device__ __forceinline__ void conn_block_row_priv(const RefArgs<O, E, W>& a, O
         }
 #pragma unroll
         for (int u = 0; u < 4; u++)
-            if (j0 + (E)u * blockDim.x < re) atomic_add(&my[a.part[v[u]]], w[u]);
+            if (j0 + (E)u * blockDim.x < re) acc_add<W>(&my[a.part[v[u]]], w[u], a.narrow);
     }
     __syncthreads();
     // merge: one thread per part sums the nw arrays (consecutive parts on
@@ -558,6 +579,9 @@ __global__ void __launch_bounds__(1024, 2) k_conn_long(RefArgs<O, E, W> a, const
     if (warp_mode) {
         part_t* keys = (part_t*)smem_raw + wid * k;
         W* vals = (W*)(smem_raw + key_bytes) + wid * k;
+        __syncthreads();  // block rows are done with the shared memory
+        for (int s = lane; s < k; s += 32) vals[s] = 0;  // conn_warp_row keeps it zero
+        __syncwarp();
         while (true) {
             O i;
             if (has_pending) {

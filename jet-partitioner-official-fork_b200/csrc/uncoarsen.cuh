@@ -47,6 +47,10 @@ struct Refiner {
     DBuf<O> s16, s32, scnt;
     O n_lorder = 0;
     mutable int long_grid_cache = -1;
+    // 1: the total edge weight of the finest level is below 2^31, so every
+    // row sum of every level fits in 32 bits (contraction only merges and
+    // drops edge weight); 0: not; -1: not yet known
+    int narrow_state = -1;
 
     struct HostState {
         W cut = 0;
@@ -123,6 +127,7 @@ struct Refiner {
         a.lock = lock.p; a.mark = mark.p; a.part = part_work.p; a.dest = dest.p; a.save_gain = save_gain.p;
         a.pregain = pregain.p; a.sizes = sizes_curr.p; a.cand = cand.p; a.cand_hub = cand_hub.p; a.moves = moves.p;
         a.moves_hub = moves_hub.p; a.dev = dev.p; a.filter = &ctl.p->filter;
+        a.narrow = narrow_state > 0 ? 1 : 0;
         return a;
     }
 
@@ -227,8 +232,22 @@ struct Refiner {
         n_lorder = (O)cnt;
     }
 
+    // Sets narrow_state from a level's total edge weight (the finest level's
+    // bounds every coarser one).
+    void set_weight_bound(const Level<O, E, W>& L) {
+        if (sizeof(W) < 8) { narrow_state = 0; return; }
+        W* sum = e.template dslot<W>(54);
+        JET_CUDA(cudaMemsetAsync(sum, 0, sizeof(int64_t), s));
+        if (L.m > 0) { k_sum<W><<<grid_persistent((int64_t)L.m, 8), BLOCK, 0, s>>>(L.val, (int64_t)L.m, sum); count_launch(); }
+        JET_LAUNCH_CHECK();
+        JET_CUDA(cudaMemcpyAsync(e.hscal, sum, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        e.sync();
+        narrow_state = (int64_t)*(W*)e.hscal < ((int64_t)1 << 31) ? 1 : 0;
+    }
+
     // init_conn_data, src/jet_refiner.hpp:958-1048.  Returns sum of capacities.
     int64_t init_conn(const Level<O, E, W>& L) {
+        if (narrow_state < 0) set_weight_bound(L);
         exclusive_scan<E, GetConnCap<O, E>>(GetConnCap<O, E>{L.row, k}, L.n, coff.p, coff.p + L.n, e.scan, s);
         JET_CUDA(cudaMemcpyAsync(&e.hscal[0], coff.p + L.n, sizeof(E), cudaMemcpyDeviceToHost, s));
         e.sync();
@@ -953,6 +972,7 @@ W uncoarsen_levels(Engine<O, E, W>& eng, const Cfg& cfg, std::vector<std::unique
     auto tr = clk::now();
     Refiner<O, E, W> ref(eng, L0.n, (int64_t)L0.m, k);
     ref.verbose = cfg.verbose;
+    ref.set_weight_bound(L0);
     part_t* cur_part = pa.p;
     part_t* other = pb.p;
     int nl = (int)levels.size();
