@@ -253,7 +253,7 @@ __device__ __forceinline__ void cta_for_row_edges(GView<O, E, W> g, const O* mem
 template <int THREADS, int SLOTS, class O, class E, class W>
 __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, const O* map, const O* list, const O* count,
                                                           const O* moff, const O* members, const E* hrow, O* skey, W* sval,
-                                                          O* ucnt, O nc) {
+                                                          O* ucnt, O nc, int narrow) {
     extern __shared__ __align__(16) unsigned char ct_smem[];
     O* keys = (O*)ct_smem;
     W* vals = (W*)(ct_smem + align16((size_t)SLOTS * sizeof(O)));
@@ -289,9 +289,9 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
                 O k = keys[slot];
                 if (k == (O)-1) {
                     O old = atomic_cas(&keys[slot], (O)-1, u);
-                    if (old == (O)-1 || old == u) { atomic_add(&vals[slot], w); return; }
+                    if (old == (O)-1 || old == u) { acc_add<W>(&vals[slot], w, narrow); return; }
                 } else if (k == u) {
-                    atomic_add(&vals[slot], w);
+                    acc_add<W>(&vals[slot], w, narrow);
                     return;
                 }
                 slot = (slot + 1) & (ts - 1);
@@ -376,7 +376,7 @@ __global__ void __launch_bounds__(THREADS) k_contract_smem(GView<O, E, W> g, con
 template <class O, class E, class W>
 __global__ void __launch_bounds__(1024) k_contract_dense(GView<O, E, W> g, const O* map, const O* list, const O* count,
                                                          const O* moff, const O* members, const E* hrow, O nc, int chunk,
-                                                         O* skey, W* sval, O* ucnt) {
+                                                         O* skey, W* sval, O* ucnt, int narrow) {
     extern __shared__ __align__(16) unsigned char ct_smem[];
     W* acc = (W*)ct_smem;
     __shared__ E s_pref[1024];
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(1024) k_contract_dense(GView<O, E, W> g, const
             __syncthreads();
             auto add = [&](E j) {
                 O u = map[g.adj[j]];
-                if (u != c && u >= base && u < top) atomic_add(&acc[u - base], g.val[j]);
+                if (u != c && u >= base && u < top) acc_add<W>(&acc[u - base], g.val[j], narrow);
             };
             if (m1 - m0 <= 32) {
                 // few members (the usual case for dense rows): stride over each member's edges

@@ -98,6 +98,17 @@ __device__ __forceinline__ int32_t atomic_add(int32_t* p, int32_t v) { return at
 __device__ __forceinline__ int64_t atomic_add(int64_t* p, int64_t v) {
     return (int64_t)atomicAdd((unsigned long long*)p, (unsigned long long)v);
 }
+
+// Adds w to a shared-memory accumulator that starts at zero.  With 64-bit
+// weights and `narrow` (the graph's total edge weight is below 2^31, so no
+// partial sum reaches 2^32) the add is a 32-bit atomic on the low word: the
+// high word stays zero and the 64-bit value is exact.  A 64-bit shared
+// atomic add costs several times as much.
+template <class W>
+__device__ __forceinline__ void acc_add(W* p, W w, int narrow) {
+    if (sizeof(W) == 8 && narrow) atomicAdd((unsigned*)p, (unsigned)w);
+    else atomic_add(p, w);
+}
 // Loads that bypass L1 so other SMs' atomics are observed within a kernel.
 template <class T> __device__ __forceinline__ T ld_cg(const T* p) { return *(const volatile T*)p; }
 template <class T> __device__ __forceinline__ void st_v(T* p, T v) { *(volatile T*)p = v; }

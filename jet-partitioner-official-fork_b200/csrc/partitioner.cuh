@@ -357,8 +357,23 @@ struct Engine {
 
     // ------------------------------------------------------------ contraction
     static constexpr int DENSE_PASSES = 8;
+    // 1: the graph being coarsened has total edge weight below 2^31, so every
+    // coarse row sum fits in 32 bits (acc_add); -1: not known yet (set from the
+    // first level contracted, which for a partition is the finest)
+    int narrow_w = -1;
+    int weight_fits_32(const Level<O, E, W>& L) {
+        if (sizeof(W) < 8) return 0;
+        W* sum = dslot<W>(55);
+        JET_CUDA(cudaMemsetAsync(sum, 0, sizeof(int64_t), s));
+        if (L.m > 0) { k_sum<W><<<grid_persistent((int64_t)L.m, 8), BLOCK, 0, s>>>(L.val, (int64_t)L.m, sum); count_launch(); }
+        JET_LAUNCH_CHECK();
+        JET_CUDA(cudaMemcpyAsync(hscal, sum, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        sync();
+        return (int64_t)*(W*)hscal < ((int64_t)1 << 31) ? 1 : 0;
+    }
     // build_coarse_graph, src/contract.hpp:347-446.
     void contract(const Level<O, E, W>& L, const O* map, O nc, Level<O, E, W>& C, DBuf<O>* skey_buf, DBuf<W>* sval_buf) {
+        if (narrow_w < 0) narrow_w = weight_fits_32(L);
         auto g = L.view();
         O n = L.n;
         DBuf<O> cnt(nc + 1, s), moff(nc + 1, s), members(n > 0 ? n : 1, s), ucnt(nc + 1, s);
@@ -409,25 +424,25 @@ struct Engine {
             JET_CUDA(cudaFuncSetAttribute(k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2a));
             k_contract_smem<CT_S1_THREADS, CT_S1_SLOTS, O, E, W><<<device_info().sms * 8, CT_S1_THREADS, sm1, s>>>(
-                g, map, l1.p, n1, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
+                g, map, l1.p, n1, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc, narrow_w); count_launch();
             JET_LAUNCH_CHECK();
             int per_sm = 0;
             JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W>,
                                                                    CT_S2A_THREADS, sm2a));
             k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W><<<device_info().sms * (per_sm > 0 ? per_sm : 1), CT_S2A_THREADS, sm2a, s>>>(
-                g, map, l2a.p, n2a, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
+                g, map, l2a.p, n2a, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc, narrow_w); count_launch();
             JET_LAUNCH_CHECK();
             JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contract_smem<CT_S2B_THREADS, CT_S2B_SLOTS, O, E, W>,
                                                                    CT_S2B_THREADS, sm2b));
             k_contract_smem<CT_S2B_THREADS, CT_S2B_SLOTS, O, E, W><<<device_info().sms * (per_sm > 0 ? per_sm : 1), CT_S2B_THREADS, sm2b, s>>>(
-                g, map, l2b.p, n2b, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
+                g, map, l2b.p, n2b, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc, narrow_w); count_launch();
             JET_LAUNCH_CHECK();
             k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W><<<device_info().sms * 2, CT_S2_THREADS, sm2, s>>>(
-                g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc); count_launch();
+                g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc, narrow_w); count_launch();
             JET_LAUNCH_CHECK();
             if (dense) {
                 k_contract_dense<O, E, W><<<device_info().sms, 1024, (size_t)dense_chunk * sizeof(W), s>>>(
-                    g, map, lh.p, nh, moff.p, members.p, hrow.p, nc, dense_chunk, skey, sval, ucnt.p); count_launch();
+                    g, map, lh.p, nh, moff.p, members.p, hrow.p, nc, dense_chunk, skey, sval, ucnt.p, narrow_w); count_launch();
                 JET_LAUNCH_CHECK();
             } else {
                 contract_hubs_sorted(g, map, lh.p, nh, moff.p, members.p, hrow.p, nc, skey, sval, ucnt.p);

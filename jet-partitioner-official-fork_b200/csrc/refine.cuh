@@ -96,16 +96,6 @@ struct RefArgs {
     int narrow;            // every row's summed edge weight fits in 32 bits (see acc_add)
 };
 
-// Adds w to a shared-memory accumulator.  With 64-bit weights and `narrow`
-// (the level's total edge weight is below 2^31, so no partial sum of a row
-// reaches 2^32) the add is a 32-bit atomic on the low word: the high word
-// stays zero and the 64-bit value is exact.  A 64-bit shared atomic add
-// costs several times as much.
-template <class W>
-__device__ __forceinline__ void acc_add(W* p, W w, int narrow) {
-    if (sizeof(W) == 8 && narrow) atomicAdd((unsigned*)p, (unsigned)w);
-    else atomic_add(p, w);
-}
 
 // ---------------------------------------------------------------- table build
 // Rows with dlo < deg <= dhi (dhi <= SET <= 32): one thread per vertex, its
@@ -1489,9 +1479,17 @@ __device__ __forceinline__ void d_mark_neighbors(RefArgs<O, E, W> a) {
             O i = a.moves[x];                                                               \
             E rs = a.g.row[i], re = a.g.row[i + 1];                                         \
             if (re - rs <= HUB_DEG)  /* hubs: one CTA each (d_mark_neighbors_hub) */         \
-                for (E j = rs + lane; j < re; j += G) {                                     \
-                    O v = a.g.adj[j];                                                       \
-                    if (!a.mark[v]) a.mark[v] = 1; /* read first: few lines get dirtied */  \
+                for (E j0 = rs + lane; j0 < re; j0 += 4 * G) {                              \
+                    /* four neighbours per lane, every load issued before the first use */  \
+                    O v[4];                                                                 \
+                    uint8_t mk[4];                                                          \
+                    _Pragma("unroll") for (int u = 0; u < 4; u++)                           \
+                        v[u] = j0 + (E)u * G < re ? a.g.adj[j0 + (E)u * G] : (O)-1;         \
+                    _Pragma("unroll") for (int u = 0; u < 4; u++)                           \
+                        mk[u] = v[u] >= 0 ? a.mark[v[u]] : (uint8_t)1;                      \
+                    /* read first: few lines get dirtied */                                 \
+                    _Pragma("unroll") for (int u = 0; u < 4; u++)                           \
+                        if (!mk[u]) a.mark[v[u]] = 1;                                       \
                 }                                                                           \
         }                                                                                   \
     }
@@ -1507,9 +1505,17 @@ __device__ __forceinline__ void d_mark_neighbors_hub(RefArgs<O, E, W> a) {
     O count = a.dev->nmoves_hub;
     for (O x = blockIdx.x; x < count; x += gridDim.x) {
         O i = a.moves_hub[x];
-        for (E j = a.g.row[i] + threadIdx.x; j < a.g.row[i + 1]; j += blockDim.x) {
-            O v = a.g.adj[j];
-            if (!a.mark[v]) a.mark[v] = 1;
+        const E re = a.g.row[i + 1];
+        for (E j0 = a.g.row[i] + threadIdx.x; j0 < re; j0 += 4 * (E)blockDim.x) {
+            O v[4];
+            uint8_t mk[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) v[u] = j0 + (E)u * blockDim.x < re ? a.g.adj[j0 + (E)u * blockDim.x] : (O)-1;
+#pragma unroll
+            for (int u = 0; u < 4; u++) mk[u] = v[u] >= 0 ? a.mark[v[u]] : (uint8_t)1;
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (!mk[u]) a.mark[v[u]] = 1;
         }
     }
 }

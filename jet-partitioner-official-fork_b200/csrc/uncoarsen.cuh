@@ -1043,6 +1043,7 @@ W run_partition(Engine<O, E, W>& eng, const Cfg& cfg, const GraphIn<O, E, W>& in
     Level<O, E, W>& L0 = *levels[0];
     L0.n = in.n; L0.m = in.m; L0.row = in.row; L0.adj = in.adj; L0.val = in.val; L0.vw = in.vw; L0.uniform = in.uniform;
     eng.prepare_level(L0);
+    eng.narrow_w = -1;  // set from this graph's finest level by the first contraction
     // coarsening cutoff, src/partitioner.hpp:88-94
     int cutoff = k * 8;
     if (cutoff > 1024) { cutoff = k * 2; cutoff = cutoff > 1024 ? cutoff : 1024; }
