@@ -50,6 +50,9 @@ WORKLOADS = {
     "rmat24": dict(desc="R-MAT 2^24, edge factor 8 (0.57/0.19/0.19/0.05), symmetrised, de-duplicated, unit weights",
                    k=256, alg=0, imb=1.10, tier="big",
                    make=lambda gr, dev: gr.rmat(24, 8, seed=1, tier="big", device=dev)),
+    "rmat22": dict(desc="R-MAT 2^22, edge factor 8 (0.57/0.19/0.19/0.05), symmetrised, de-duplicated, unit weights",
+                   k=256, alg=0, imb=1.10, tier="big",
+                   make=lambda gr, dev: gr.rmat(22, 8, seed=1, tier="big", device=dev)),
     "rmat18": dict(desc="R-MAT 2^18, edge factor 8 (0.57/0.19/0.19/0.05), symmetrised, de-duplicated, unit weights",
                    k=256, alg=0, imb=1.10, tier="big",
                    make=lambda gr, dev: gr.rmat(18, 8, seed=1, tier="big", device=dev)),
@@ -212,10 +215,14 @@ def _hbm_peak():
 
 
 def run_only(args, wl, local):
-    """Connectivity-table build (init_conn_data) alone on the finest graph
-    with a fixed random k-way partition: the library's CUDA events around the
-    table-build kernels of each call, inputs resident, L2 flushed between
-    calls."""
+    """Connectivity-table build (init_conn_data) alone on one level of the
+    workload: the finest graph, or with --level-max-n N the first level of at
+    most N vertices of the workload's own coarsening (the library's
+    coarsen_map + contract).  The partition is a fixed random k-way one, or
+    with --part refined the library's partition of that level.  The
+    library's CUDA events bracket the table-build kernels of each call;
+    inputs resident, L2 flushed between calls; the last call runs inside an
+    NVTX range "conn_build" (for ncu --nvtx-include "conn_build/")."""
     import torch
 
     torch.cuda.set_device(local)
@@ -223,28 +230,44 @@ def run_only(args, wl, local):
     dev = torch.device("cuda", local)
     g = wl["make"](jet.graphs, dev)
     k = wl["k"]
-    gen = torch.Generator(device=dev).manual_seed(1)
-    part = torch.randint(0, k, (g.n,), generator=gen, device=dev, dtype=torch.int32)
+    level = 1
+    while args.level_max_n > 0 and g.n > args.level_max_n:
+        cmap, nc, _ = jet.coarsen_map(g, wl["alg"], level=level, seed=1)
+        g = jet.contract(g, cmap, nc)
+        level += 1
+    if args.part == "refined":
+        cfg = jet.config_t(coarsening_alg=wl["alg"], num_parts=k, max_imb_ratio=wl["imb"])
+        part, _, _ = getattr(jet, PART_FN[wl["tier"]])(cfg, g, seed=1)
+        part = part.to(torch.int32)
+    else:
+        gen = torch.Generator(device=dev).manual_seed(1)
+        part = torch.randint(0, k, (g.n,), generator=gen, device=dev, dtype=torch.int32)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream(dev)
     for _ in range(args.warmup):
         jet.conn_build(g, part, k)
     times, nbytes, slots = [], 0.0, 0
-    for _ in range(args.steps):
+    for step in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
+        last = step == args.steps - 1
+        if last:
+            torch.cuda.nvtx.range_push("conn_build")
         # the library's own CUDA events bracket exactly the table-build kernels
         jet.prof_enable(True)
         off, ent, val, size = jet.conn_build(g, part, k)
         prof = jet.prof_read()["conn_build"]
         jet.prof_enable(False)
+        if last:
+            torch.cuda.nvtx.range_pop()
         times.append(prof["ms"])
         nbytes = prof["bytes"]
         slots = int(off[-1].item())
     ms = statistics.median(times)
     peak = _hbm_peak()["value"]
     achieved = nbytes / (ms / 1000.0) / 1e9
-    print(json.dumps({"kernel": "conn_build", "workload": args.workload, "n": g.n, "nnz": g.nnz, "k": k, "slots": slots,
+    print(json.dumps({"kernel": "conn_build", "workload": args.workload, "level_max_n": args.level_max_n, "part": args.part,
+                      "n": g.n, "nnz": g.nnz, "k": k, "slots": slots,
                       "ms_median": ms, "algorithmic_bytes": nbytes, "achieved_gbs": achieved, "peak_gbs": peak,
                       "frac": achieved / peak, "steps": args.steps}), flush=True)
 
@@ -454,7 +477,11 @@ def main():
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--powerlaw-scale", type=int, default=24, help="R-MAT scale of the power-law run (0 = skip)")
     ap.add_argument("--only", default=None, choices=["conn_build"],
-                    help="time one kernel alone on the workload's finest graph (profiling case)")
+                    help="time one kernel alone on one level of the workload (profiling case)")
+    ap.add_argument("--level-max-n", type=int, default=0,
+                    help="--only: coarsen to the first level of at most this many vertices (0 = finest)")
+    ap.add_argument("--part", default="random", choices=["random", "refined"],
+                    help="--only: a random k-way partition or the library's partition of the level")
     args = ap.parse_args()
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_env()
