@@ -1689,6 +1689,7 @@ __global__ void __launch_bounds__(1024) k_finalize_ctl(RefArgs<O, E, W> a, Ctl<W
     ctl_set_handles(c, h, true);
 }
 
+
 // ---------------------------------------------------------------- statistics
 // Cut counted from both endpoints (src/part_stat.hpp:77-108).
 template <int G, class O, class E, class W>

@@ -363,37 +363,66 @@ struct Refiner {
         JET_LAUNCH_CHECK();
     }
 
-    // perform_moves, src/jet_refiner.hpp:905-955: every kernel up to the
-    // cut change from the updated tables.
-    void moves_kernels(const Level<O, E, W>& L) {
+    // perform_moves, src/jet_refiner.hpp:905-955, in four parts: the moves
+    // themselves (apply_moves_kernel, which also decides update_small versus
+    // update_large), the small update (subtract pass over all moved vertices,
+    // hubs included, then the add pass), the large update (mark the
+    // neighbours, rebuild their tables) and the cut change.  Both updates'
+    // kernels test the device-side decision, so running both is correct.
+    void apply_moves_kernel(const Level<O, E, W>& L) {
         auto a = args(L);
         int hist = (size_t)k * sizeof(W) <= 32 * 1024;
         k_apply_moves<O, E, W><<<grid_persistent(L.n, 8), BLOCK, hist ? (size_t)k * sizeof(W) : 0, s>>>(a, hist); count_launch();
         JET_LAUNCH_CHECK();
-        int h = prof_begin(s);
+    }
+    void small_update_kernels(const Level<O, E, W>& L) {
+        auto a = args(L);
+        unsigned grid = grid_persistent((int64_t)L.n * L.group / 4 + 1, 16);
+        const unsigned hub_grid = device_info().sms * 2;
+        // every subtraction before any addition (src/jet_refiner.hpp:786, :810)
+        switch (L.group) {
+            case 4: k_update_small<4, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 8: k_update_small<8, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 16: k_update_small<16, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            default: k_update_small<32, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+        }
+        count_launch();
+        if (L.n_hub > 0) { k_update_small_hub<false, O, E, W><<<hub_grid, 1024, 0, s>>>(a); count_launch(); }
+        switch (L.group) {
+            case 4: k_update_small<4, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 8: k_update_small<8, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 16: k_update_small<16, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            default: k_update_small<32, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+        }
+        count_launch();
+        if (L.n_hub > 0) { k_update_small_hub<true, O, E, W><<<hub_grid, 1024, 0, s>>>(a); count_launch(); }
+        JET_LAUNCH_CHECK();
+    }
+    void large_update_kernels(const Level<O, E, W>& L) {
+        auto a = args(L);
         unsigned grid = grid_persistent((int64_t)L.n * L.group / 4 + 1, 16);
         switch (L.group) {
-            case 4: k_update_small<4, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); k_update_small<4, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch();
-                    k_mark_neighbors<4, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
-            case 8: k_update_small<8, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); k_update_small<8, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch();
-                    k_mark_neighbors<8, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
-            case 16: k_update_small<16, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); k_update_small<16, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch();
-                     k_mark_neighbors<16, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
-            default: k_update_small<32, false, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); k_update_small<32, true, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch();
-                     k_mark_neighbors<32, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
+            case 4: k_mark_neighbors<4, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 8: k_mark_neighbors<8, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            case 16: k_mark_neighbors<16, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
+            default: k_mark_neighbors<32, O, E, W><<<grid, BLOCK, 0, s>>>(a); break;
         }
+        count_launch();
+        if (L.n_hub > 0) { k_mark_neighbors_hub<O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch(); }
         JET_LAUNCH_CHECK();
-        if (L.n_hub > 0) {
-            // the subtract pass must finish before any add: two launches
-            k_update_small_hub<false, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch();
-            k_update_small_hub<true, O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch();
-            k_mark_neighbors_hub<O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch();
-            JET_LAUNCH_CHECK();
-        }
         build_tables(L, 1, &dev.p->large);
-        prof_end(h, PK_UPDATE, 0, s);
-        k_cut_after<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(a); count_launch();
+    }
+    void cut_after_kernel(const Level<O, E, W>& L) {
+        k_cut_after<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(args(L)); count_launch();
         JET_LAUNCH_CHECK();
+    }
+    void moves_kernels(const Level<O, E, W>& L) {
+        apply_moves_kernel(L);
+        int h = prof_begin(s);
+        small_update_kernels(L);
+        large_update_kernels(L);
+        prof_end(h, PK_UPDATE, 0, s);
+        cut_after_kernel(L);
     }
 
     // Host-driven iteration end: results to pinned memory, one host sync.
@@ -773,6 +802,9 @@ struct Refiner {
             capture_into(b_weak, {}, [&] { weak(L, pb.opt, pb.size_max); }, &kw);
             cudaGraphNode_t n_strong = add_conditional(body, {n_weak}, h.strong, cudaGraphCondTypeIf, &b_strong);
             capture_into(b_strong, {}, [&] { strong(L, pb.opt, pb.size_max); }, &ks);
+            // (the update_small / update_large kernels all run and test the
+            // device-side decision: conditional nodes around them cost more
+            // than the kernels that return at once)
             auto tm = capture_into(body, {n_strong}, [&] {
                 moves_kernels(L);
                 k_finalize_ctl<O, E, W><<<1, 1024, 0, s>>>(args(L), cp, h); count_launch();
