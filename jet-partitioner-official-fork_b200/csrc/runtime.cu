@@ -502,7 +502,9 @@ int jet_set_refine_drivers(int mask) { return g_drivers.exchange(mask & JET_DRIV
 // levels).  They also wait on streams without
 // spinning and send Metis calls to helper processes.
 void jet_thread_batch_mode(int on) {
-    t_driver_mask = on ? JET_DRIVER_CTA : JET_DRIVER_ALL;
+    // one CTA for small levels, a 16-CTA cluster for mid-size ones (it needs
+    // 16 SMs, not the whole GPU), the host loop above
+    t_driver_mask = on ? (JET_DRIVER_CTA | JET_DRIVER_CLUSTER) : JET_DRIVER_ALL;
     t_batch = on != 0;
 }
 

@@ -554,10 +554,12 @@ struct Refiner {
     // ------------------------------------------------------------ single-CTA loop
     // Levels above CTA_PREFER_N vertices run faster on a 16-CTA cluster when
     // one is available (measured on meshes: 77 vs 127 us per iteration at
-    // 4k vertices, 82 vs 104 in favour of one CTA at 835).
+    // 4k vertices, 82 vs 104 in favour of one CTA at 835).  Batch and server
+    // workers keep one CTA up to CTA_MAX_N: with many partitions sharing the
+    // GPU, one SM per level gives more throughput than sixteen.
     static constexpr int64_t CTA_PREFER_N = 2048;
     bool cta_eligible(const Level<O, E, W>& L) const {
-        int64_t cap = (use_cluster && cluster_size() > 0) ? CTA_PREFER_N : CTA_MAX_N;
+        int64_t cap = (use_cluster && !batch_thread() && cluster_size() > 0) ? CTA_PREFER_N : CTA_MAX_N;
         return use_cta && (int64_t)L.n <= cap && (int64_t)L.m <= CTA_MAX_M && k <= CTA_MAX_K;
     }
 
