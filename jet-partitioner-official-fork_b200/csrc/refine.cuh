@@ -807,17 +807,40 @@ __global__ void __launch_bounds__(BLOCK) k_lp_select_warp(RefArgs<O, E, W> a, co
 // src/jet_refiner.hpp:275-307: a candidate keeps its move if its gain,
 // recomputed assuming every higher-priority candidate (larger pre-gain, then
 // smaller id) has already moved, is non-negative.
+// A candidate's gain change from its edges j0, j0 + stride, ... < e: an
+// edge to a higher-priority neighbour v counts -w / +w for v's destination
+// and +w / -w for v's current part being the candidate's part p / best.
+// Four edges per round, with every round's loads (neighbours, weights, their
+// pregains, then their destinations and parts where needed) issued before
+// the first use.
 template <class O, class E, class W>
-__device__ __forceinline__ W afterburn_edge(const RefArgs<O, E, W>& a, O i, W igain, part_t p, part_t best, E j) {
-    O v = a.g.adj[j];
-    W vgain = a.pregain[v];
+__device__ __forceinline__ W afterburn_edges(const RefArgs<O, E, W>& a, O i, W igain, part_t p, part_t best, E j0, E e, E stride) {
     W ch = 0;
-    if (vgain > igain || (vgain == igain && v < i)) {
-        W w = a.g.val[j];
-        part_t vp = a.dest[v];
-        if (vp == p) ch -= w; else if (vp == best) ch += w;
-        vp = a.part[v];
-        if (vp == p) ch += w; else if (vp == best) ch -= w;
+    for (; j0 < e; j0 += 4 * stride) {
+        O v[4];
+        W w[4], vg[4];
+        part_t vd[4], vp[4];
+        bool take[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const E j = j0 + (E)u * stride;
+            v[u] = j < e ? a.g.adj[j] : (O)-1;
+            w[u] = j < e ? a.g.val[j] : (W)0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) vg[u] = v[u] >= 0 ? a.pregain[v[u]] : (W)0;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            take[u] = v[u] >= 0 && (vg[u] > igain || (vg[u] == igain && v[u] < i));
+            vd[u] = take[u] ? a.dest[v[u]] : NULL_PART;
+            vp[u] = take[u] ? a.part[v[u]] : NULL_PART;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (!take[u]) continue;
+            if (vd[u] == p) ch -= w[u]; else if (vd[u] == best) ch += w[u];
+            if (vp[u] == p) ch += w[u]; else if (vp[u] == best) ch -= w[u];
+        }
     }
     return ch;
 }
@@ -834,7 +857,7 @@ __device__ __forceinline__ void d_afterburn(RefArgs<O, E, W> a) {
             igain = a.pregain[i]; p = a.part[i]; best = a.dest[i];                          \
         }                                                                                   \
         W ch = 0;                                                                           \
-        if (act) for (E j = s + lane; j < e; j += G) ch += afterburn_edge<O, E, W>(a, i, igain, p, best, j); \
+        if (act) ch = afterburn_edges<O, E, W>(a, i, igain, p, best, s + lane, e, (E)G);   \
         ch = group_sum<W>(ch, G);                                                           \
         bool keep = act && lane == 0 && igain + ch >= 0;                                    \
         if (keep) a.lock[i] = 1;                                                            \
@@ -857,7 +880,7 @@ __device__ __forceinline__ void d_afterburn_hub(RefArgs<O, E, W> a) {
         W igain = a.pregain[i];
         part_t p = a.part[i], best = a.dest[i];
         W ch = 0;
-        for (E j = a.g.row[i] + threadIdx.x; j < a.g.row[i + 1]; j += blockDim.x) ch += afterburn_edge<O, E, W>(a, i, igain, p, best, j);
+        ch = afterburn_edges<O, E, W>(a, i, igain, p, best, a.g.row[i] + threadIdx.x, a.g.row[i + 1], (E)blockDim.x);
         ch = group_sum<W>(ch, 32);
         if ((threadIdx.x & 31) == 0) part_sum[threadIdx.x >> 5] = ch;
         __syncthreads();
