@@ -55,6 +55,28 @@ __device__ __forceinline__ void argmax_merge(W& bw, E& bj, W w2, E j2) {
     if (j2 >= 0 && (bj < 0 || w2 > bw || (w2 == bw && j2 > bj))) { bw = w2; bj = j2; }
 }
 
+// Heaviest eligible edge among j0, j0 + stride, ... < e (argmax_merge is a
+// total order, so the edge order does not matter), four edges per round with
+// the neighbour ids, weights and neighbour weights all loaded before the first use.
+template <class O, class E, class W>
+__device__ __forceinline__ void heavy_edges(const GView<O, E, W>& g, W max_allowed, E j0, E e, E stride, W& bw, E& bj) {
+    for (; j0 < e; j0 += 4 * stride) {
+        O v[4];
+        W w[4], vw[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const E j = j0 + (E)u * stride;
+            v[u] = j < e ? g.adj[j] : (O)-1;
+            w[u] = j < e ? g.val[j] : (W)0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) vw[u] = v[u] >= 0 ? g.vw[v[u]] : max_allowed;
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (vw[u] < max_allowed) argmax_merge<O, E, W>(bw, bj, w[u], j0 + (E)u * stride);
+    }
+}
+
 template <int G, class O, class E, class W>
 __global__ void __launch_bounds__(BLOCK) k_hec_heavy(GView<O, E, W> g, const W* vsum, O* hn) {
     W max_allowed = (W)(6 * (*vsum)) / (W)g.n;
@@ -65,11 +87,7 @@ __global__ void __launch_bounds__(BLOCK) k_hec_heavy(GView<O, E, W> g, const W* 
         bool act = false;                                                                   \
         if (in) { s = g.row[i]; e = g.row[i + 1]; act = (e - s) > 0 && (e - s) <= HUB_DEG && g.vw[i] < max_allowed; } \
         W bw = 0; E bj = -1;                                                                \
-        if (act)                                                                            \
-            for (E j = s + lane; j < e; j += G) {                                           \
-                O v = g.adj[j];                                                             \
-                if (g.vw[v] < max_allowed) argmax_merge<O, E, W>(bw, bj, g.val[j], j);      \
-            }                                                                               \
+        if (act) heavy_edges<O, E, W>(g, max_allowed, s + lane, e, (E)G, bw, bj);          \
         for (int m = G >> 1; m > 0; m >>= 1) {                                              \
             W w2 = shfl_xor(bw, m, G); E j2 = shfl_xor(bj, m, G);                           \
             argmax_merge<O, E, W>(bw, bj, w2, j2);                                          \
@@ -320,6 +338,36 @@ __device__ __forceinline__ bool pick_skip(O u, const O* vcmap, const O* hn) {
     return vcmap[u] != MAXV || hn[u] == MAXV || vcmap[hn[u]] == MAXV;
 }
 
+// The best (weight, hash, edge) of a vertex's eligible edges j0, j0 + stride,
+// ... < e (pick_better's total order, so the edge order does not matter),
+// four edges per round with the neighbour ids, weights and match states all
+// loaded before the first use.
+template <bool INITIAL, bool UNIFORM, class O, class E, class W>
+__device__ __forceinline__ void pick_edges(const GView<O, E, W>& g, const O* vcmap, uint32_t r, E j0, E e, E stride, int64_t& bw,
+                                           uint32_t& bh, int64_t& bj) {
+    const O MAXV = ord_max<O>();
+    for (; j0 < e; j0 += 4 * stride) {
+        O v[4];
+        int64_t w[4];
+        bool ok[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const E j = j0 + (E)u * stride;
+            v[u] = j < e ? g.adj[j] : (O)-1;
+            w[u] = (!UNIFORM && j < e) ? (int64_t)g.val[j] : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) ok[u] = v[u] >= 0 && (INITIAL || vcmap[v[u]] == MAXV);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (!ok[u]) continue;
+            const uint32_t h = xorshift32((uint32_t)((uint64_t)v[u] + r));
+            const int64_t j = (int64_t)(j0 + (E)u * stride);
+            if (pick_better(w[u], h, j, bw, bh, bj)) { bw = w[u]; bh = h; bj = j; }
+        }
+    }
+}
+
 template <int G, bool INITIAL, bool UNIFORM, class O, class E, class W>
 __global__ void __launch_bounds__(BLOCK) k_pick_match(GView<O, E, W> g, const O* perm, const O* perm_len, const O* vcmap, O* hn,
                                                       uint64_t seed, uint64_t stream) {
@@ -335,15 +383,7 @@ __global__ void __launch_bounds__(BLOCK) k_pick_match(GView<O, E, W> g, const O*
             r = (uint32_t)jet_rng(seed, stream, (uint64_t)u);                               \
         }                                                                                   \
         int64_t bw = 0; uint32_t bh = 0; int64_t bj = -1;                                   \
-        if (act)                                                                            \
-            for (E j = s + lane; j < e; j += G) {                                           \
-                O v = g.adj[j];                                                             \
-                if (INITIAL || vcmap[v] == MAXV) {                                          \
-                    int64_t w = UNIFORM ? 0 : (int64_t)g.val[j];                            \
-                    uint32_t h = xorshift32((uint32_t)((uint64_t)v + r));                   \
-                    if (pick_better(w, h, (int64_t)j, bw, bh, bj)) { bw = w; bh = h; bj = j; } \
-                }                                                                           \
-            }                                                                               \
+        if (act) pick_edges<INITIAL, UNIFORM, O, E, W>(g, vcmap, r, s + lane, e, (E)G, bw, bh, bj); \
         for (int m = G >> 1; m > 0; m >>= 1) {                                              \
             int64_t w2 = shfl_xor(bw, m, G); uint32_t h2 = shfl_xor(bh, m, G);              \
             int64_t j2 = shfl_xor(bj, m, G);                                                \
@@ -368,15 +408,7 @@ __global__ void __launch_bounds__(1024) k_pick_match_hub(GView<O, E, W> g, const
         if (!INITIAL && act) act = vcmap[u] == MAXV && hn[u] != MAXV;
         uint32_t r = (uint32_t)jet_rng(seed, stream, (uint64_t)u);
         int64_t bw = 0; uint32_t bh = 0; int64_t bj = -1;
-        if (act)
-            for (E j = g.row[u] + threadIdx.x; j < g.row[u + 1]; j += blockDim.x) {
-                O v = g.adj[j];
-                if (INITIAL || vcmap[v] == MAXV) {
-                    int64_t w = UNIFORM ? 0 : (int64_t)g.val[j];
-                    uint32_t h = xorshift32((uint32_t)((uint64_t)v + r));
-                    if (pick_better(w, h, (int64_t)j, bw, bh, bj)) { bw = w; bh = h; bj = j; }
-                }
-            }
+        if (act) pick_edges<INITIAL, UNIFORM, O, E, W>(g, vcmap, r, g.row[u] + threadIdx.x, g.row[u + 1], (E)blockDim.x, bw, bh, bj);
         for (int m = 16; m > 0; m >>= 1) {
             int64_t w2 = shfl_xor(bw, m, 32); uint32_t h2 = shfl_xor(bh, m, 32); int64_t j2 = shfl_xor(bj, m, 32);
             if (pick_better(w2, h2, j2, bw, bh, bj)) { bw = w2; bh = h2; bj = j2; }
