@@ -361,6 +361,35 @@ __global__ void __launch_bounds__(BLOCK) k_scan_apply(Get get, int64_t n, const 
     }
 }
 
+// Small scans in one launch: one 1024-thread block walks the input in chunks
+// of 4096 (four items per thread) with a running carry.
+static constexpr int64_t SCAN_ONE_BLOCK_MAX = 16384;
+template <class T, class Get>
+__global__ void __launch_bounds__(1024) k_scan_one(Get get, int64_t n, T* out, T* total) {
+    __shared__ T sw[32];
+    T carry = 0;
+    for (int64_t base = 0; base < n; base += 4 * 1024) {
+        T v[4];
+        T s = 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int64_t i = base + (int64_t)threadIdx.x * 4 + j;
+            v[j] = i < n ? get(i) : T(0);
+            s += v[j];
+        }
+        T tot;
+        T ex = block_exclusive_scan<T>(s, sw, tot) + carry;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int64_t i = base + (int64_t)threadIdx.x * 4 + j;
+            if (i < n) out[i] = ex;
+            ex += v[j];
+        }
+        carry += tot;
+    }
+    if (threadIdx.x == 0 && total) *total = carry;
+}
+
 template <class T>
 struct GetArray {
     const T* a;
@@ -382,6 +411,11 @@ template <class T, class Get>
 inline void exclusive_scan(Get get, int64_t n, T* out, T* total, ScanScratch& sc, cudaStream_t s) {
     if (n <= 0) {
         if (total) JET_CUDA(cudaMemsetAsync(total, 0, sizeof(T), s));
+        return;
+    }
+    if (n <= SCAN_ONE_BLOCK_MAX) {
+        k_scan_one<T, Get><<<1, 1024, 0, s>>>(get, n, out, total); count_launch();
+        JET_LAUNCH_CHECK();
         return;
     }
     int64_t ntiles = ceil_div<int64_t>(n, SCAN_TILE);
