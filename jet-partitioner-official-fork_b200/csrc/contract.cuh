@@ -430,6 +430,22 @@ __global__ void __launch_bounds__(1024) k_contract_dense(GView<O, E, W> g, const
 // row by a five-step binary search over the lanes (shuffles); loads and
 // stores stay coalesced.
 static constexpr int CT_COPY_CHUNK = 2048;
+// The same packing with one warp per row, for levels whose rows are all
+// short (no row above 2048 member edges): no row search, one pass.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_contract_copy_rows(O nc, const E* hrow, const O* skey, const W* sval, const E* crow,
+                                                             O* cadj, W* cval) {
+#define CC_BODY(x, in, lane)                                                                \
+    {                                                                                       \
+        if (in) {                                                                           \
+            const O c = (O)x;                                                               \
+            const E hs = hrow[c], o = crow[c], cnt = crow[c + 1] - o;                      \
+            for (E t = lane; t < cnt; t += 32) { cadj[o + t] = skey[hs + t]; cval[o + t] = sval[hs + t]; } \
+        }                                                                                   \
+    }
+    JET_GROUP_LOOP(32, nc, CC_BODY)
+#undef CC_BODY
+}
 template <class O, class E>
 __global__ void k_copy_chunk_rows(O nc, const E* crow, O* chunk_row) {
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nc; c += (int64_t)gridDim.x * blockDim.x) {

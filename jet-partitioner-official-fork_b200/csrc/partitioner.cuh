@@ -460,8 +460,16 @@ struct Engine {
         C.m = mc;
         C.own_adj.alloc(mc > 0 ? mc : 1, s);
         C.own_val.alloc(mc > 0 ? mc : 1, s);
-        // every row's unique entries are packed at its scratch offset, in neighbour order
-        if (mc > 0) {
+        // every row's unique entries are packed at its scratch offset, in
+        // neighbour order; rows of at most 2048 member edges only (the
+        // counts of the two largest bins are zero): one warp per row
+        const bool short_rows = *(O*)&hscal[1] == 0 && *(O*)&hscal[2] == 0;
+        if (mc > 0 && short_rows) {
+            k_contract_copy_rows<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(nc, hrow.p, skey, sval, C.own_row.p,
+                                                                                              C.own_adj.p, C.own_val.p);
+            count_launch();
+            JET_LAUNCH_CHECK();
+        } else if (mc > 0) {
             const int64_t chunks = ((int64_t)mc + CT_COPY_CHUNK - 1) / CT_COPY_CHUNK;
             DBuf<O> chunk_row(chunks, s);
             k_copy_chunk_rows<O, E><<<grid_persistent(nc, 8), BLOCK, 0, s>>>(nc, C.own_row.p, chunk_row.p); count_launch();
