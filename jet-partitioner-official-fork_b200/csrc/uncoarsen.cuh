@@ -201,7 +201,8 @@ struct Refiner {
     // levels with fewer rows of degree > THREAD_DEG keep the per-list kernels
     static constexpr int64_t LONG_MIN_ROWS = 1024;
     // 1024 threads, two blocks per SM (measured against 512 x 4: faster on
-    // levels dominated by single-warp rows, even on whole-block rows)
+    // levels dominated by single-warp rows, about 10% slower on a level of
+    // whole-block rows, which are rarer)
     int long_threads() const { return 1024; }
     int long_grid() const {
         if (long_grid_cache >= 0) return long_grid_cache;
