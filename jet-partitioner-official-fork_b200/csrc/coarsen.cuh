@@ -127,48 +127,6 @@ __global__ void __launch_bounds__(1024) k_hec_heavy_hub(GView<O, E, W> g, const 
     }
 }
 
-// One aggregation round of parallel_map_construct (src/heuristics.hpp:101-126):
-// lock-free claims with compare-and-swap; the `swap` parity breaks stalls.
-template <class O>
-__global__ void k_hec_round(O n, const O* perm, const O* perm_len, const O* hn, O* vcmap, int swap) {
-    const O MAXV = ord_max<O>();
-    O len = perm ? *perm_len : n;
-    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < len; x += (int64_t)gridDim.x * blockDim.x) {
-        O u = perm ? perm[x] : (O)x;
-        O v = hn[u];
-        int condition = u < v;
-        if (condition ^ swap) {
-            if (atomic_cas(&vcmap[u], MAXV, MAXV - 1) == MAXV) {
-                if (u == v || atomic_cas(&vcmap[v], MAXV, MAXV - 1) == MAXV) {
-                    O cv = v < u ? v : u;
-                    st_v(&vcmap[u], cv);
-                    st_v(&vcmap[v], cv);
-                } else {
-                    O t = ld_cg(&vcmap[v]);
-                    st_v(&vcmap[u], t < n ? t : MAXV);
-                }
-            }
-        }
-    }
-}
-
-// Keeps the vertices still unsettled (vcmap >= n) for the next round.
-template <class O>
-__global__ void k_hec_compact(O n, const O* perm, const O* perm_len, const O* vcmap, O* next, O* next_len) {
-    O len = perm ? *perm_len : n;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    int64_t start = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    int64_t rounds = ceil_div<int64_t>((int64_t)len, stride);
-    for (int64_t r = 0; r < rounds; r++) {
-        int64_t x = start + r * stride;
-        O u = 0;
-        bool keep = false;
-        if (x < len) { u = perm ? perm[x] : (O)x; keep = ld_cg(&vcmap[u]) >= n; }
-        O s = warp_append(next_len, keep);
-        if (keep) next[s] = u;
-    }
-}
-
 // ---------------------------------------------------------------- HEC, in-order semantics
 // The reference's aggregation rounds (src/heuristics.hpp:101-126) executed in
 // index order settle every vertex within two rounds, and both rounds have a

@@ -107,9 +107,6 @@ __device__ __forceinline__ void cta_zero_buckets(const RebArgs<O, W>& rb) {
     __syncthreads();
 }
 
-template <int G, class O, class E, class W>
-__device__ __forceinline__ void cta_afterburn(RefArgs<O, E, W>& a) { d_afterburn<G, O, E, W>(a); }
-
 template <class O, class E, class W>
 __global__ void __launch_bounds__(CTA_THREADS, 1)
 k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, W> rbs, Ctl<W>* c, part_t* best_part,
