@@ -400,3 +400,43 @@ def test_contract_wide_id_range_rows(jet, graphs, orc, tier):
     assert np.array_equal(host(got.adj), want.adj)
     assert np.array_equal(host(got.val), want.val)
     assert np.array_equal(host(got.vw), want.vw)
+
+
+@pytest.mark.parametrize("tier", ["big", "biggest"])
+def test_wide_weights_exact(jet, graphs, orc, tier):
+    """Edge weights of 2^26 to 2^27 (total far above 2^31): the shared-memory
+    accumulators must take the 64-bit path, not the 32-bit one.  Tables,
+    contraction and refinement iterations equal the oracle's."""
+    g = make(graphs, "dense", "i32")
+    gen = torch.Generator().manual_seed(12)
+    und = torch.randint(1 << 26, 1 << 27, (g.nnz,), generator=gen, dtype=torch.int64)
+    # symmetric weights: the weight of (u, v) and (v, u) from the smaller endpoint's edge index
+    src = torch.repeat_interleave(torch.arange(g.n), (g.row[1:] - g.row[:-1]).long())
+    dst = g.adj.long()
+    key = torch.minimum(src, dst) * g.n + torch.maximum(src, dst)
+    _, inv = torch.unique(key, return_inverse=True)
+    w = und[inv]
+    g = graphs.CSRGraph(g.n, g.row, g.adj, w, g.vw.to(torch.int64), False, "i32").as_tier(tier)
+    og = orc.G.from_csr(g)
+    assert int(w.sum()) > (1 << 31)
+    for k in (64, 300):
+        part = (np.arange(g.n) % k).astype(np.int32)
+        off, ent, val, size = orc.conn_build(og, part, k)
+        goff, gent, gval, gsize = jet.conn_build(g.to("cuda"), torch.from_numpy(part).cuda(), k)
+        assert np.array_equal(host(gsize), size)
+        assert table_multisets(host(goff), host(gent), host(gval), host(gsize)) == table_multisets(off, ent, val, size)
+    m = (np.arange(g.n) // 2).astype(np.int64 if tier == "biggest" else np.int32)
+    want = orc.contract(og, m, g.n // 2)
+    got = jet.contract(g.to("cuda"), torch.from_numpy(m).cuda(), g.n // 2)
+    assert np.array_equal(host(got.row), want.row) and np.array_equal(host(got.adj), want.adj)
+    assert np.array_equal(host(got.val), want.val)
+    part = (np.arange(g.n) % 64).astype(np.int32)
+    part[: g.n // 3] = 0  # badly unbalanced: rebalancing iterations with large updates
+    for iters in (1, 3, 6):
+        want = orc.refine_iters(og, part, 64, 1.03, 0.75, iters)
+        got = jet.refine_iters(g.to("cuda"), torch.from_numpy(part).cuda(), 64, 1.03, 0.75, iters)
+        assert got["kinds"] == list(want["kinds"])
+        assert np.array_equal(host(got["part"]), want["part"])
+        assert got["cut"] == want["cut"]
+        gm = table_multisets(host(got["off"]), host(got["ent"]), host(got["val"]), host(got["size"]))
+        assert gm == table_multisets(want["off"], want["ent"], want["val"], want["size"])
