@@ -47,6 +47,8 @@ WORKLOADS = {
                       tier="i32", make=lambda gr, dev: gr.grid3d(128, 128, 128, weighted=True, seed=1, tier="i32", device=dev)),
     "grid2d256": dict(desc="2D 4-neighbour grid 256x256, unit weights", k=32, alg=1, imb=1.03, tier="i32",
                       make=lambda gr, dev: gr.grid2d(256, 256, weighted=False, tier="i32", device=dev)),
+    "grid2d256": dict(desc="2D 4-point grid 256^2, unit weights", k=32, alg=1, imb=1.03, tier="i32",
+                      make=lambda gr, dev: gr.grid2d(256, 256, weighted=False, seed=1, device=dev)),
     "rmat24": dict(desc="R-MAT 2^24, edge factor 8 (0.57/0.19/0.19/0.05), symmetrised, de-duplicated, unit weights",
                    k=256, alg=0, imb=1.10, tier="big",
                    make=lambda gr, dev: gr.rmat(24, 8, seed=1, tier="big", device=dev)),
