@@ -9,7 +9,7 @@
 // Parity status: UNPINNED.  The reference ships no tests, fixtures or golden
 // vectors, and it cannot be compiled here (it needs Kokkos and KokkosKernels,
 // neither of which is available), so this restatement is checked only against
-// hand-derived known answers and invariants (tests/test_oracle_*.py).
+// hand-derived known answers and invariants (tests/test_oracle.py).
 //
 // Semantics follow the reference executed on one thread (its Serial execution
 // space): every "parallel" loop runs in index order and every atomic is a plain
