@@ -1658,7 +1658,8 @@ __global__ void k_ctl_begin(Ctl<W>* c, CtlHandles h) {
 // next mode, and resets the per-iteration counters.
 template <class O, class W>
 __device__ __forceinline__ void ctl_end_logic(Ctl<W>* c, RefDev<O, W>* d, W mx) {
-    c->curr_cut -= d->cut1 + d->cut2;
+    // the cut changes were summed by other blocks' atomics: read past L1
+    c->curr_cut -= ld_cg(&d->cut1) + ld_cg(&d->cut2);
     c->curr_imb = mx > c->opt ? mx - c->opt : 0;
     c->copy = 0;
     if (c->best_imb > c->imb_max && c->curr_imb < c->best_imb) {
@@ -1708,6 +1709,28 @@ template <class O, class E, class W>
 __global__ void __launch_bounds__(1024) k_finalize_ctl(RefArgs<O, E, W> a, Ctl<W>* c, CtlHandles h) {
     W mx = block_max_sizes<W>(a.sizes, a.k);
     if (threadIdx.x != 0) return;
+    ctl_end_logic<O, W>(c, a.dev, mx);
+    ctl_set_handles(c, h, true);
+}
+
+// k_cut_after and k_finalize_ctl in one launch (one graph node less per
+// iteration): every block adds its cut change, and the last block to finish
+// (a counter, reset by that block) closes the iteration.
+template <class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_cut_finalize_ctl(RefArgs<O, E, W> a, Ctl<W>* c, CtlHandles h, unsigned* done) {
+    __shared__ int s_last;
+    d_cut_after<O, E, W>(a);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    W mx = block_max_sizes<W>(a.sizes, a.k);
+    if (threadIdx.x != 0) return;
+    *done = 0;
     ctl_end_logic<O, W>(c, a.dev, mx);
     ctl_set_handles(c, h, true);
 }

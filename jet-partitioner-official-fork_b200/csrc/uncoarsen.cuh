@@ -45,6 +45,7 @@ struct Refiner {
     DBuf<unsigned> lctr;
     // rows of 9-16 and of 17-32 edges (per level) and their counts
     DBuf<O> s16, s32, scnt;
+    DBuf<unsigned> cdone;  // k_cut_finalize_ctl's block counter
     O n_lorder = 0;
     mutable int long_grid_cache = -1;
     // 1: the total edge weight of the finest level is below 2^31, so every
@@ -83,6 +84,8 @@ struct Refiner {
         s16.alloc(n1, s);
         s32.alloc(n1, s);
         scnt.alloc(2, s);
+        cdone.alloc(1, s);
+        cdone.zero();
         lctr.alloc(2, s);
         lctr.zero();
         dev.alloc(1, s);
@@ -809,8 +812,12 @@ struct Refiner {
             // device-side decision: conditional nodes around them cost more
             // than the kernels that return at once)
             auto tm = capture_into(body, {n_strong}, [&] {
-                moves_kernels(L);
-                k_finalize_ctl<O, E, W><<<1, 1024, 0, s>>>(args(L), cp, h); count_launch();
+                apply_moves_kernel(L);
+                int hp = prof_begin(s);
+                small_update_kernels(L);
+                large_update_kernels(L);
+                prof_end(hp, PK_UPDATE, 0, s);
+                k_cut_finalize_ctl<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(args(L), cp, h, cdone.p); count_launch();
                 JET_LAUNCH_CHECK();
             }, &km);
             add_conditional(body, tm, h.copy, cudaGraphCondTypeIf, &b_copy);
