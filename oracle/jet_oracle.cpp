@@ -6,10 +6,15 @@
 // only tests, the smoke check and the benchmark's CPU-baseline leg may load it.
 // Nothing in the product links or calls it.
 //
-// Parity status: UNPINNED.  The reference ships no tests, fixtures or golden
-// vectors, and it cannot be compiled here (it needs Kokkos and KokkosKernels,
-// neither of which is available), so this restatement is checked only against
-// hand-derived known answers and invariants (tests/test_oracle.py).
+// Parity status: PINNED to the reference's own code.  oracle/ref.mk compiles
+// the unmodified reference sources against a host-only Kokkos stand-in
+// (oracle/kokkos_shim/) into oracle/_ref/, and tests/test_ref_pin.py runs
+// every step below through both and demands identical results: pstat,
+// gain_bucket, contraction given a map, connectivity tables given a partition,
+// coarsening maps, LP / weak / strong refinement iterations, a full refinement
+// level and uncoarsening a fixed hierarchy (the last four with edge weights
+// under which no two parts tie, since ties are broken differently -- below),
+// plus the 8-seed median cut within 2% of the reference's.
 //
 // Semantics follow the reference executed on one thread (its Serial execution
 // space): every "parallel" loop runs in index order and every atomic is a plain
@@ -1048,6 +1053,36 @@ orc::Csr<O, E, W> make_csr(int64_t n, const void* row, const void* adj, const vo
     return g;
 }
 
+// uncoarsener::multilevel_jet (src/uncoarsen.hpp:88-125): refine each level,
+// coarsest first, then project onto the next finer level.  `part` holds the
+// coarsest level's partition on entry and the finest level's on exit.
+template <class O, class E, class W>
+bool uncoarsen_levels(const std::vector<orc::Level<O, E, W>>& levels, const orc_config* cfg,
+                      std::vector<orc::part_t>& part, orc::State<O, E, W>& best, orc_stats* st) {
+    using namespace orc;
+    part_t k = cfg->num_parts;
+    Refiner<O, E, W> ref(levels[0].g.n, k);
+    int nl = (int)levels.size();
+    bool ok = true;
+    for (int l = nl - 1; l >= 0; l--) {
+        LevelRecord rec;
+        ok = ref.refine(levels[l].g, levels[l].vw.data(), k, cfg->max_imb_ratio, cfg->refine_tolerance,
+                        cfg->ultra_settings != 0, levels[l].uniform, part.data(), best, &rec, cfg->verbose != 0) && ok;
+        if (st && nl - 1 - l < 256) {
+            int idx = nl - 1 - l;
+            st->level_cut[idx] = rec.cut_half; st->level_n[idx] = rec.n; st->level_nnz[idx] = rec.nnz;
+            st->level_iters[idx] = rec.iters; st->level_lp_iters[idx] = rec.lp_iters;
+        }
+        if (l > 0) {
+            const std::vector<O>& map = levels[l].map;
+            std::vector<part_t> fine(levels[l - 1].g.n);
+            for (size_t i = 0; i < fine.size(); i++) fine[i] = part[map[i]];
+            part.swap(fine);
+        }
+    }
+    return ok;
+}
+
 // partitioner::partition, src/partitioner.hpp:61-125, with contracter::
 // generate_coarse_graphs (src/contract.hpp:494-533) and uncoarsener::
 // uncoarsen (src/uncoarsen.hpp:88-158).
@@ -1086,26 +1121,8 @@ int run_partition(const orc_config* cfg, int64_t n, const void* row, const void*
     std::vector<part_t> part(coarsest.g.n, 0);
     if (metis_init(coarsest.g, coarsest.vw.data(), k, cfg->max_imb_ratio, part.data()) != 0) return 3;
     auto t2 = clk::now();
-    Refiner<O, E, W> ref(levels[0].g.n, k);
     State<O, E, W> best;
-    int nl = (int)levels.size();
-    bool ok = true;
-    for (int l = nl - 1; l >= 0; l--) {
-        LevelRecord rec;
-        ok = ref.refine(levels[l].g, levels[l].vw.data(), k, cfg->max_imb_ratio, cfg->refine_tolerance,
-                        cfg->ultra_settings != 0, levels[l].uniform, part.data(), best, &rec, cfg->verbose != 0) && ok;
-        if (st && nl - 1 - l < 256) {
-            int idx = nl - 1 - l;
-            st->level_cut[idx] = rec.cut_half; st->level_n[idx] = rec.n; st->level_nnz[idx] = rec.nnz;
-            st->level_iters[idx] = rec.iters; st->level_lp_iters[idx] = rec.lp_iters;
-        }
-        if (l > 0) {
-            const std::vector<O>& map = levels[l].map;
-            std::vector<part_t> fine(levels[l - 1].g.n);
-            for (size_t i = 0; i < fine.size(); i++) fine[i] = part[map[i]];
-            part.swap(fine);
-        }
-    }
+    bool ok = uncoarsen_levels(levels, cfg, part, best, st);
     auto t3 = clk::now();
     std::copy(part.begin(), part.end(), part_out);
     *cut_out = (int64_t)(best.cut / 2);
@@ -1116,7 +1133,7 @@ int run_partition(const orc_config* cfg, int64_t n, const void* row, const void*
         st->largest = (int64_t)largest;
         st->smallest = (int64_t)smallest;
         st->imb = (double)largest / (double)optimal_size<O>((O)best.total_size, k);
-        st->levels = nl;
+        st->levels = (int32_t)levels.size();
         st->coarsest_n = (int32_t)coarsest.g.n;
         st->t_coarsen = secs(t0, t1); st->t_init = secs(t1, t2); st->t_refine = secs(t2, t3); st->t_total = secs(t0, t3);
     }
@@ -1251,6 +1268,32 @@ int orc_refine_level(int tier, int64_t n, const void* row, const void* adj, cons
         bool ok = ref.refine(g, (const W*)vw, k, imb, tol, false, uniform_ew != 0, part, st, &rec, false);
         *cut_out = (int64_t)st.cut;
         if (iters_out) *iters_out = rec.iters;
+        return ok ? 0 : 4;
+    });
+}
+
+// uncoarsener::uncoarsen (src/uncoarsen.hpp:127-158) over a fixed hierarchy,
+// as the reference's jet_import app does (app/import_coarse.cpp:49-132).
+// Level 0 is the finest; maps[l] (l >= 1) sends level l-1's vertices to level
+// l.  coarsest_part has ns[nlevels-1] entries; part_out receives ns[0];
+// *cut_out counts each cut edge once.
+int orc_uncoarsen(int tier, int nlevels, const int64_t* ns, const void* const* rows, const void* const* adjs,
+                  const void* const* vals, const void* const* vws, const void* const* maps,
+                  const int32_t* coarsest_part, const orc_config* cfg, int uniform_finest, int32_t* part_out,
+                  int64_t* cut_out) {
+    ORC_TIER_DISPATCH(tier, {
+        std::vector<orc::Level<O, E, W>> levels(nlevels);
+        for (int l = 0; l < nlevels; l++) {
+            levels[l].g = make_csr<O, E, W>(ns[l], rows[l], adjs[l], vals[l]);
+            levels[l].vw.assign((const W*)vws[l], (const W*)vws[l] + ns[l]);
+            levels[l].uniform = (l == 0) && uniform_finest;
+            if (l > 0) levels[l].map.assign((const O*)maps[l], (const O*)maps[l] + ns[l - 1]);
+        }
+        std::vector<orc::part_t> part(coarsest_part, coarsest_part + ns[nlevels - 1]);
+        orc::State<O, E, W> best;
+        bool ok = uncoarsen_levels(levels, cfg, part, best, nullptr);
+        std::copy(part.begin(), part.end(), part_out);
+        *cut_out = (int64_t)(best.cut / 2);
         return ok ? 0 : 4;
     });
 }

@@ -1,8 +1,8 @@
 """ctypes wrapper around the CPU oracle (oracle/jet_oracle.cpp).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
-benchmark's CPU-baseline and reference legs.  Parity status: unpinned (the
-reference has no golden vectors and cannot be built here without Kokkos).
+benchmark's CPU-baseline leg.  Parity status: pinned to the reference's own
+code built under oracle/_ref/ (oracle/ref.py, tests/test_ref_pin.py).
 """
 from __future__ import annotations
 
@@ -200,3 +200,24 @@ def gain_bucket(gain: int, vwgt: int, wide: bool = False) -> int:
 
 def rng(seed: int, stream: int, idx: int) -> int:
     return int(lib().orc_rng(seed, stream, idx))
+
+
+def uncoarsen(levels, maps, coarsest_part, k: int, imb: float = 1.03, tol: float = 0.999, ultra: bool = False):
+    """Refines a fixed hierarchy (levels[0] finest, maps[l] sends level l-1 to
+    level l, maps[0] unused) from a coarsest partition.  Returns (part, cut)."""
+    tier = levels[0].tier
+    nl = len(levels)
+    ns = np.array([lv.n for lv in levels], dtype=np.int64)
+    arr = lambda xs: (ctypes.c_void_p * nl)(*[ctypes.c_void_p(x.ctypes.data) if x is not None else None for x in xs])
+    od = TIER_DT[tier][0]
+    mp = [None] + [np.ascontiguousarray(m, dtype=od) for m in maps[1:]]
+    cp = np.ascontiguousarray(coarsest_part, dtype=np.int32)
+    cfg = OrcConfig(1, k, imb, tol, int(ultra), 0)
+    part = np.zeros(levels[0].n, dtype=np.int32)
+    cut = ctypes.c_int64(0)
+    rc = lib().orc_uncoarsen(tier, nl, _p(ns), arr([lv.row for lv in levels]), arr([lv.adj for lv in levels]),
+                             arr([lv.val for lv in levels]), arr([lv.vw for lv in levels]), arr(mp), _p(cp),
+                             ctypes.byref(cfg), int(levels[0].uniform), _p(part), ctypes.byref(cut))
+    if rc != 0:
+        raise RuntimeError("oracle uncoarsen failed with code %d" % rc)
+    return part, int(cut.value)
