@@ -12,9 +12,10 @@ uniform in [1, 10] from seed 1), k = 64, HEC coarsening, imbalance 1.03.
 With --gpus N > 1 (launched by torch.distributed.run) every rank partitions
 its own replica of the graph (independent work, no collective on the data
 path); the value is the whole job's graphs/s over the max-over-ranks time.
---impl reference times the CPU oracle (a restatement of the reference's
-algorithm; the reference itself needs Kokkos and cannot be built here) on the
-host cores, rank 0 only.
+--impl reference times the reference's own CPU path -- its unmodified
+sources built against a host-only Kokkos stand-in (oracle/ref.mk), run as
+its jet_host (OpenMP) configuration on every host core -- on the same graph,
+rank 0 only.
 """
 from __future__ import annotations
 
@@ -45,8 +46,6 @@ def load_pkg():
 WORKLOADS = {
     "grid3d128": dict(desc="3D 7-point grid 128^3, edge weights uniform in [1,10] (seed 1)", k=64, alg=1, imb=1.03,
                       tier="i32", make=lambda gr, dev: gr.grid3d(128, 128, 128, weighted=True, seed=1, tier="i32", device=dev)),
-    "grid2d256": dict(desc="2D 4-neighbour grid 256x256, unit weights", k=32, alg=1, imb=1.03, tier="i32",
-                      make=lambda gr, dev: gr.grid2d(256, 256, weighted=False, tier="i32", device=dev)),
     "grid2d256": dict(desc="2D 4-point grid 256^2, unit weights", k=32, alg=1, imb=1.03, tier="i32",
                       make=lambda gr, dev: gr.grid2d(256, 256, weighted=False, seed=1, device=dev)),
     "rmat24": dict(desc="R-MAT 2^24, edge factor 8 (0.57/0.19/0.19/0.05), symmetrised, de-duplicated, unit weights",
@@ -59,16 +58,15 @@ WORKLOADS = {
                    k=256, alg=0, imb=1.10, tier="big",
                    make=lambda gr, dev: gr.rmat(18, 8, seed=1, tier="big", device=dev)),
 }
-# DRAM bytes (read + write) per algorithmic byte from one ncu capture of the
-# class's largest launch (profiles/k_conn_thread_grid3d128_k64.md); the
-# per-launch traffic reported is this ratio times the per-launch algorithmic
-# bytes of the timed region.
+# DRAM bytes (read + write) per algorithmic byte of the finest-level table
+# build on the 128^3 grid, from one ncu capture of that launch (134.9 MB read
+# + 71.1 MB written against 283.2 MB algorithmic).  A constant: DRAM traffic
+# cannot be measured outside ncu; the reported per-launch traffic is this
+# ratio times the per-launch algorithmic bytes of the timed region.
 NCU_TRAFFIC_RATIO = {
-    "conn_build": {"grid3d128": {"ratio": (134.903552 + 71.064320) / 283.246592,
-                                 "note": "ncu dram bytes of the finest-level launch (206.0 MB of 283.2 MB algorithmic), "
-                                         "scaled to the per-launch average"}},
     "conn_build_finest": {"grid3d128": {"ratio": (134.903552 + 71.064320) / 283.246592,
-                                        "note": "ncu dram bytes (read + write) of the finest-level launch"}},
+                                        "note": "constant: ncu DRAM bytes (read + write) of one finest-level launch "
+                                                "per algorithmic byte, times this run's algorithmic bytes"}},
 }
 ALG_NAME = {0: "2-hop matching", 1: "HEC", 2: "matching"}
 PART_FN = {"i32": "partition", "big": "partition_big", "biggest": "partition_biggest"}
@@ -136,72 +134,114 @@ def dist_env():
     return ws, rank, local
 
 
-def oracle_partition(g, wl, seed):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+def _oracle_mods():
+    """The CPU checker modules: the oracle (oracle/jet_oracle.cpp) and the
+    reference's own code built under oracle/_ref/ (oracle/ref.py)."""
+    path = os.path.join(ROOT, "oracle")
+    if path not in sys.path:
+        sys.path.insert(0, path)
     import oracle
-    og = oracle.G.from_csr(g.to("cpu"))
-    t = time.perf_counter()
-    part, cut, st = oracle.partition(og, wl["k"], alg=wl["alg"], imb=wl["imb"], seed=seed)
-    return time.perf_counter() - t, cut, st.imb
+    import ref
+    return oracle, ref
 
 
-_REF_STATE = {}
+def host_graph(g):
+    """A graph's arrays on the host in the checkers' form."""
+    oracle, _ = _oracle_mods()
+    return oracle.G.from_csr(g.to("cpu"))
 
 
-def _ref_init(workload):
-    """Worker set-up for the CPU arm: the workload's graph in the oracle's form."""
-    jet = load_pkg()
-    wl = WORKLOADS[workload]
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    g = wl["make"](jet.graphs, "cpu")
-    _REF_STATE.update(og=oracle.G.from_csr(g), oracle=oracle, wl=wl)
-
-
-def _ref_partition(seed):
-    st = _REF_STATE
-    t = time.perf_counter()
-    part, cut, info = st["oracle"].partition(st["og"], st["wl"]["k"], alg=st["wl"]["alg"], imb=st["wl"]["imb"], seed=seed)
-    return time.perf_counter() - t, cut, info.imb
+def reference_partition(og, wl, seed, space="host"):
+    """One partition by the reference's own code: (seconds of the partition
+    call, cut, imbalance)."""
+    _, ref = _oracle_mods()
+    part, cut, imb, secs = ref.partition(og, wl["k"], alg=wl["alg"], imb=wl["imb"], seed=seed, space=space)
+    return secs, cut, imb
 
 
 def run_reference(args, wl, rank):
-    """CPU arm: the oracle (a restatement of the reference's algorithm; the
-    reference itself needs Kokkos and cannot be built here) on every host
-    core, one independent partition per core per step (one graph is
-    partitioned by one thread, so the cores run replicas with different
-    seeds); graphs/s = partitions finished / wall time."""
+    """CPU arm: the reference's own jet_host path (its unmodified sources on
+    the host-only Kokkos stand-in, OpenMP over every host core) partitions the
+    workload's graph once per step; graphs/s = steps / summed partition time.
+    The graph is built on the host with the same generator and seed as the
+    GPU arm's, so both partition the same graph."""
     if rank != 0:
         return
-    import multiprocessing as mp
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    oracle, ref = _oracle_mods()
     jet = load_pkg()
     g = wl["make"](jet.graphs, "cpu")
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores, initializer=_ref_init, initargs=(args.workload,)) as pool:
-        for s in range(args.warmup):
-            pool.map(_ref_partition, [100 + s * cores + c for c in range(cores)])
-        walls, cuts, imbs = [], [], []
-        for s in range(args.steps):
-            t = time.perf_counter()
-            res = pool.map(_ref_partition, [1 + s * cores + c for c in range(cores)])
-            walls.append(time.perf_counter() - t)
-            cuts += [r[1] for r in res]
-            imbs += [r[2] for r in res]
-    total = sum(walls)
-    value = args.steps * cores / total
+    og = oracle.G.from_csr(g)
+    cores = ref.concurrency("host")
+    for s in range(args.warmup):
+        reference_partition(og, wl, 100 + s)
+    secs, cuts, imbs = [], [], []
+    for s in range(args.steps):
+        dt, cut, imb = reference_partition(og, wl, 1 + s)
+        secs.append(dt)
+        cuts.append(cut)
+        imbs.append(imb)
+    total = sum(secs)
+    value = args.steps / total
     line = {
         "impl": "reference", "metric": "graphs/sec", "value": value, "unit": "graphs/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": wl["tier"], "data": "synthetic",
         "config": config_of(args, wl, g),
         "edges_per_s": value * g.nnz / 2, "cut_median": statistics.median(cuts), "imbalance_max": max(imbs),
-        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": cores, "kind": "port",
-                         "sample": "%d steps of %d concurrent full partitions (one per host core, oracle/jet_oracle.cpp)"
-                                   % (args.steps, cores)},
+        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": cores, "kind": "reference",
+                         "sample": "%d full partitions of the workload's graph, one after another, each by the "
+                                   "reference's jet_host path on %d OpenMP threads" % (args.steps, cores)},
         "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+_BATCH_REF = {}
+
+
+def _batch_ref_init(path):
+    _oracle_mods()
+    _BATCH_REF["dir"] = path
+
+
+def _batch_ref_one(i):
+    """One batched-config graph through the reference's Serial build (one
+    host core): the arrays come from files the parent wrote."""
+    import numpy as np
+    oracle, ref = _oracle_mods()
+    d = _BATCH_REF["dir"]
+    arr = [np.load(os.path.join(d, "%d_%s.npy" % (i, nm))) for nm in ("row", "adj", "val", "vw")]
+    k = int(np.load(os.path.join(d, "%d_k.npy" % i)))
+    og = oracle.G(*arr, uniform=False)
+    t = time.perf_counter()
+    _, cut, _, _ = ref.partition(og, k, alg=1, imb=1.03, seed=i + 1, space="serial")
+    return time.perf_counter() - t, cut
+
+
+def run_batched_cpu(gs, cfgs, cores):
+    """The batched config on the host: the reference's single-thread build
+    partitions the same graphs, one graph per host core at a time (a pool of
+    `cores` processes); graphs/s = graphs / wall time."""
+    import multiprocessing as mp
+    import shutil
+    import numpy as np
+    tmp = tempfile.mkdtemp(prefix="jet_batch_")
+    try:
+        for i, (g, c) in enumerate(zip(gs, cfgs)):
+            for nm, a in zip(("row", "adj", "val", "vw"), g.numpy()):
+                np.save(os.path.join(tmp, "%d_%s.npy" % (i, nm)), a)
+            np.save(os.path.join(tmp, "%d_k.npy" % i), np.int64(c.num_parts))
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(cores, initializer=_batch_ref_init, initargs=(tmp,)) as pool:
+            pool.map(_batch_ref_one, list(range(min(cores, len(gs)))))  # warm-up: libraries loaded
+            t0 = time.perf_counter()
+            res = pool.map(_batch_ref_one, list(range(len(gs))), chunksize=1)
+            wall = time.perf_counter() - t0
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return {"value": len(gs) / wall, "unit": "graphs/s", "cores": cores, "kind": "reference",
+            "sample": "all %d graphs, each partitioned by the reference's Serial build on one host core, %d at a "
+                      "time" % (len(gs), cores), "wall_s": wall, "cuts": [r[1] for r in res]}
 
 
 def _hbm_peak():
@@ -298,12 +338,14 @@ def max_over_ranks(x, ws, dist, device):
     return float(t.item())
 
 
-def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None):
+def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None, cpu_cores=0):
     """Plain (one graph per call, one after another) against the batched
     executor on the same graphs; wall clock with the device synchronised on
     both sides (the batched run spans many streams).  With several ranks the
     graphs are sharded by longest-processing-time first and each rank runs
-    its own shard; times are the slowest rank's."""
+    its own shard; times are the slowest rank's.  With cpu_cores > 0 (one
+    rank) the reference's own code partitions the same graphs on the host
+    as the CPU baseline."""
     import torch
     specs = batched_specs(count)
     owner = jet.assign_lpt([n for n, _ in specs], ws)
@@ -330,7 +372,12 @@ def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None):
     equal = max_over_ranks(0.0 if all(r[1] == p for r, p in zip(res, plain)) else 1.0, ws, dist, dev) == 0.0
     lat = sorted(r[2] for r in res) or [0.0]
     edges = sum(g.nnz for g in gs) // 2
-    return {"graphs": count, "graphs_this_rank": len(mine), "workers": workers,
+    cpu = None
+    if cpu_cores > 0 and ws == 1:
+        cpu = run_batched_cpu(gs, cfgs, cpu_cores)
+        cpu_cuts = cpu.pop("cuts")
+        cpu["cut_ratio_median"] = statistics.median(r[1] / max(c, 1) for r, c in zip(res, cpu_cuts))
+    return {"cpu_baseline": cpu, "graphs": count, "graphs_this_rank": len(mine), "workers": workers,
             "sum_vertices_this_rank": sum(g.n for g in gs), "undirected_edges_this_rank": edges,
             "plain_graphs_per_s": count / t_plain, "batched_graphs_per_s": count / t_batch,
             "speedup": t_plain / t_batch, "equal_cut": equal,
@@ -338,12 +385,53 @@ def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None):
             "timing": "wall clock, device synchronised before and after; max over ranks"}
 
 
-def run_powerlaw(jet, dev, scale, steps=2):
+POWERLAW = dict(k=256, alg=0, imb=1.10, tier="big")
+
+
+def start_oracle_check(jet, dev, scale):
+    """Starts the oracle's partition of R-MAT 2^scale (the power-law config at
+    a size one host thread finishes in well under a minute) on a background
+    thread; the GPU's partition of the same graph is compared with it at the
+    end of the power-law run.  The oracle call releases the interpreter lock,
+    so it overlaps the GPU work that follows."""
+    import threading
+    g = jet.graphs.rmat(scale, 8, seed=1, tier="big", device=dev)
+    og = host_graph(g)
+    oracle, _ = _oracle_mods()
+    out = {}
+
+    def work():
+        t = time.perf_counter()
+        out["part"], out["cut"], _ = oracle.partition(og, POWERLAW["k"], alg=POWERLAW["alg"], imb=POWERLAW["imb"],
+                                                      seed=1)
+        out["seconds"] = time.perf_counter() - t
+
+    th = threading.Thread(target=work, daemon=True)
+    th.start()
+    return {"graph": g, "scale": scale, "thread": th, "out": out}
+
+
+def finish_oracle_check(jet, chk):
+    import numpy as np
+    cfg = jet.config_t(coarsening_alg=POWERLAW["alg"], num_parts=POWERLAW["k"], max_imb_ratio=POWERLAW["imb"])
+    part, cut, _ = jet.partition_big(cfg, chk["graph"], seed=1)
+    chk["thread"].join()
+    o = chk["out"]
+    return {"graph": "R-MAT 2^%d, edge factor 8, k = 256, 2-hop, imbalance 1.10, seed 1" % chk["scale"],
+            "n": chk["graph"].n, "undirected_edges": chk["graph"].nnz // 2, "gpu_cut": cut, "oracle_cut": o["cut"],
+            "partition_equal": bool(np.array_equal(part.cpu().numpy(), o["part"])) and cut == o["cut"],
+            "oracle_seconds_one_thread": o["seconds"]}
+
+
+def run_powerlaw(jet, dev, scale, steps=2, cpu_scale=0, check=None):
     """The power-law config: R-MAT 2^scale (edge factor 8, symmetrised,
     de-duplicated, unit weights), int64 offsets and weights, 2-hop matching,
     k = 256, imbalance 1.10.  One warm-up and `steps` timed partitions with
     the graph resident in HBM (CUDA events); edges/s per phase is the sum of
-    the level edge counts over the phase's time."""
+    the level edge counts over the phase's time.  cpu_scale > 0 times the
+    reference's jet_host path on R-MAT 2^cpu_scale (a bounded sample of the
+    same generator) as the CPU baseline in edges/s; `check` is a started
+    oracle comparison (start_oracle_check)."""
     import torch
     g = jet.graphs.rmat(scale, 8, seed=1, tier="big", device=dev)
     cfg = jet.config_t(coarsening_alg=0, num_parts=256, max_imb_ratio=1.10)
@@ -378,7 +466,19 @@ def run_powerlaw(jet, dev, scale, steps=2):
                       "levels": v["launches"]}
     m = {k: v for k, v in zip(jet.MEASUREMENT_NAMES, exp.measurements)}
     sum_m = sum(cl.numEdges for cl in exp.coarseLevels) / 2
-    return {"workload": "rmat%d" % scale, "n": g.n, "undirected_edges": g.nnz // 2, "k": 256, "coarsening": "2-hop matching",
+    cpu = None
+    if cpu_scale > 0:
+        _, ref = _oracle_mods()
+        gs = jet.graphs.rmat(cpu_scale, 8, seed=1, tier="big", device=dev)
+        ogs = host_graph(gs)
+        del gs
+        dt, ccut, cimb = reference_partition(ogs, POWERLAW, 1)
+        cpu = {"value": float(ogs.row[-1] / 2) / dt, "unit": "edges/s", "cores": ref.concurrency("host"), "kind": "reference",
+               "sample": "one partition of R-MAT 2^%d (same generator and settings, %d undirected edges) by the "
+                         "reference's jet_host path, %.1f s" % (cpu_scale, ogs.row[-1] // 2, dt),
+               "gpu_edges_per_s": (g.nnz / 2) / (statistics.median(times) / 1000.0)}
+    chk = finish_oracle_check(jet, check) if check is not None else None
+    return {"cpu_baseline": cpu, "oracle_check": chk, "workload": "rmat%d" % scale, "n": g.n, "undirected_edges": g.nnz // 2, "k": 256, "coarsening": "2-hop matching",
             "imbalance": 1.10, "tier": "big", "ms_per_partition": statistics.median(times), "steps": steps,
             "edges_per_s": (g.nnz / 2) / (statistics.median(times) / 1000.0), "cut": cut, "imbalance_ratio": exp.imb_ratio,
             "levels": len(exp.coarseLevels),
@@ -473,11 +573,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="grid3d128", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--batched", type=int, default=512, help="graphs in the batched comparison (0 = skip)")
     ap.add_argument("--serving", type=int, default=96, help="requests in the serving run (0 = skip)")
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--powerlaw-scale", type=int, default=24, help="R-MAT scale of the power-law run (0 = skip)")
+    ap.add_argument("--check-scale", type=int, default=20,
+                    help="R-MAT scale of the power-law GPU-against-oracle partition check (0 = skip)")
     ap.add_argument("--only", default=None, choices=["conn_build"],
                     help="time one kernel alone on one level of the workload (profiling case)")
     ap.add_argument("--level-max-n", type=int, default=0,
@@ -566,9 +668,18 @@ def main():
     h2d = (g.n + 1) * eb + g.nnz * (ob + wb) + g.n * wb
     d2h = g.n * 4
     e2e_value = ws * len(e2e_times) / sum(e2e_times) if e2e_times else None
-    batched = run_batched(jet, dev, args.batched, args.workers, ws, rank, dist) if args.batched > 0 else None
+    cpu_cores = 0
+    if ws == 1 and not args.no_cpu_baseline:
+        cpu_cores = _oracle_mods()[1].concurrency("host")
+    chk = None
+    if args.powerlaw_scale > 0 and args.check_scale > 0 and rank == 0:
+        chk = start_oracle_check(jet, dev, args.check_scale)
+    batched = run_batched(jet, dev, args.batched, args.workers, ws, rank, dist, cpu_cores) if args.batched > 0 else None
     serving = run_serving(jet, dev, args.serving, args.workers, 120 << 30) if args.serving > 0 and rank == 0 else None
-    powerlaw = run_powerlaw(jet, dev, args.powerlaw_scale) if args.powerlaw_scale > 0 and rank == 0 else None
+    powerlaw = None
+    if args.powerlaw_scale > 0 and rank == 0:
+        powerlaw = run_powerlaw(jet, dev, args.powerlaw_scale, cpu_scale=(args.powerlaw_scale - 3) if cpu_cores else 0,
+                                check=chk)
 
     if rank != 0:
         if ws > 1:
@@ -601,9 +712,10 @@ def main():
                 "launches": cb["launches"]}
     cpu_base = None
     if ws == 1 and not args.no_cpu_baseline:
-        dt, ocut, oimb = oracle_partition(g, wl, seed=1)
-        cpu_base = {"value": 1.0 / dt, "unit": "graphs/s", "cores": 1, "kind": "port",
-                    "sample": "one full partition of the same graph on one host thread (oracle/jet_oracle.cpp), cut %d" % ocut}
+        dt, ocut, oimb = reference_partition(host_graph(g), wl, 1)
+        cpu_base = {"value": 1.0 / dt, "unit": "graphs/s", "cores": cpu_cores, "kind": "reference",
+                    "sample": "one full partition of the same graph by the reference's jet_host path on %d OpenMP "
+                              "threads, cut %d" % (cpu_cores, ocut)}
     sorted_t = sorted(times)
     line = {
         "metric": "graphs/sec", "value": value, "unit": "graphs/s", "n_gpus": ws, "steps": args.steps,

@@ -230,17 +230,21 @@ int jet_pstat(int tier, int64_t n, int64_t nnz, const void* row_map, const void*
 int jet_project(int tier, int64_t n_fine, const void* map, const int32_t* coarse, int32_t* fine, void* stream);
 
 /* Same results as jet_pstat, for callers that must not trigger any device
- * allocation: code recording into a CUDA stream capture (where cudaMalloc is
- * illegal) and services that reserve device memory up front and forbid the
- * library from allocating later.  No counterpart in the reference.
- * Scratch is a fixed array of about 256 KiB that the library reserves on every
- * GPU that loads it, held until the process exits.  Limits: num_parts k <= 16384
- * (JET_ERR_INVALID beyond), part ids must lie in [0, k).  The first call on a
- * device looks up the array's device address; make that first call before
- * any stream capture.  Every call shares the array, so calls that overlap on
- * the GPU (different streams, no ordering between them) race and must be
- * serialised by the caller.  Graph arrays and part[] are device pointers;
- * out[6] is host memory; stream NULL means the legacy default stream. */
+ * allocation: services that reserve the GPU's memory up front for their own
+ * pool (a caching allocator holding the whole device, a real-time loop that
+ * must never enter the driver's allocator) and forbid the library from
+ * allocating later.  No counterpart in the reference.
+ * Scratch is a fixed array of about 256 KiB in the library's device module,
+ * held by every GPU that loads it until the process exits.  Under CUDA's lazy
+ * module loading (the default) the module -- and the array's memory -- is
+ * loaded by the first call on each device, which also looks up the array's
+ * device address: make that first call (or set CUDA_MODULE_LOADING=EAGER)
+ * before reserving the rest of the device's memory.  Limits: num_parts k <=
+ * 16384 (JET_ERR_INVALID beyond), part ids must lie in [0, k).  Every call
+ * shares the array, so calls that overlap on the GPU (different streams, no
+ * ordering between them) race and must be serialised by the caller.  Graph
+ * arrays and part[] are device pointers; out[6] is host memory (the call waits
+ * for its stream); stream NULL means the legacy default stream. */
 int jet_pstat_noalloc(int tier, int64_t n, int64_t nnz, const void* row_map, const void* entries, const void* values,
                       const void* vweights, const int32_t* part, int32_t k, int64_t* out, void* stream);
 

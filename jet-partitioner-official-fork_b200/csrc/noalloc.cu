@@ -2,15 +2,19 @@
 //
 // jet_pstat computes the pstat quantities (cut, largest per-part cut,
 // communication volume, part sizes) with scratch memory it allocates per
-// call.  Some callers cannot let a library allocate device memory:
-//   * code that records its GPU work into a CUDA stream capture, where
-//     cudaMalloc is not a legal operation;
-//   * services that reserve all device memory up front for their own pool
-//     (a framework's caching allocator, a real-time loop that must never
-//     block inside the driver's allocator) and forbid allocation afterwards.
-// jet_pstat_noalloc serves them: its scratch lives in the file-scope array
-// below, reserved once when the library is loaded (every GPU that loads the
-// library holds it until the process exits), so a call allocates nothing.
+// call.  Some callers cannot let a library allocate device memory: services
+// that reserve the GPU's memory up front for their own pool (a framework's
+// caching allocator that has taken the whole device, a real-time loop that
+// must never block inside the driver's allocator) and forbid allocation
+// afterwards.  jet_pstat_noalloc serves them: its scratch lives in the
+// file-scope array below, which every GPU that loads this module holds until
+// the process exits, so a call allocates nothing.
+//
+// Under CUDA's lazy module loading (the default since CUDA 12) the module,
+// and with it the array's device memory, is loaded on the first call on each
+// device, which also looks up the array's device address.  That first call
+// (or running with CUDA_MODULE_LOADING=EAGER) must therefore come before the
+// caller reserves the rest of the device's memory.
 #include "api_impl.cuh"
 #include <climits>
 #include <mutex>
@@ -120,16 +124,29 @@ static long long* scratch_ptr(int* status) {
     static long long* ptrs[64] = {};
     static std::mutex mu;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) { *status = JET_ERR_CUDA; return nullptr; }
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        set_last_error("jet_pstat_noalloc: no usable current device");
+        *status = JET_ERR_CUDA;
+        return nullptr;
+    }
     std::lock_guard<std::mutex> lk(mu);
     if (!ptrs[dev]) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e != cudaSuccess || !p) { *status = JET_ERR_CUDA; return nullptr; }
+        if (e != cudaSuccess || !p) {
+            set_last_error(std::string("jet_pstat_noalloc: scratch array lookup failed: ") + cudaGetErrorString(e));
+            *status = JET_ERR_CUDA;
+            return nullptr;
+        }
         ptrs[dev] = (long long*)p;
     }
     *status = JET_OK;
     return ptrs[dev];
+}
+
+static int cuda_fail(const char* where, cudaError_t e) {
+    set_last_error(std::string("jet_pstat_noalloc: ") + where + ": " + cudaGetErrorString(e));
+    return JET_ERR_CUDA;
 }
 
 template <class O, class E, class W>
@@ -138,7 +155,8 @@ static int run(int64_t n, int64_t nnz, const void* row, const void* adj, const v
     int st = JET_OK;
     long long* scr = scratch_ptr(&st);
     if (st != JET_OK) return st;
-    if (cudaMemsetAsync(scr, 0, sizeof(long long) * (8 + 2 * (size_t)MAX_PARTS), s) != cudaSuccess) return JET_ERR_CUDA;
+    cudaError_t e = cudaMemsetAsync(scr, 0, sizeof(long long) * (8 + 2 * (size_t)MAX_PARTS), s);
+    if (e != cudaSuccess) return cuda_fail("clearing the scratch array", e);
     if (n > 0) {
         int sms = device_info().sms;
         int64_t blocks = (n + WARPS - 1) / WARPS;
@@ -146,15 +164,19 @@ static int run(int64_t n, int64_t nnz, const void* row, const void* adj, const v
         k_pstat_na<O, E, W><<<(unsigned)blocks, WARPS * 32, 0, s>>>((O)n, (const E*)row, (const O*)adj, (const W*)val,
                                                                     (const W*)vw, part, k, scr);
         count_launch();
-        if (cudaGetLastError() != cudaSuccess) return JET_ERR_CUDA;
+        if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail("statistics kernel launch", e);
     }
     k_pstat_na_final<<<1, 1024, 0, s>>>(k, scr);
     count_launch();
-    if (cudaGetLastError() != cudaSuccess) return JET_ERR_CUDA;
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail("final reduction launch", e);
     long long res[7];
-    if (cudaMemcpyAsync(res, scr + 8 + 2 * MAX_PARTS, sizeof(res), cudaMemcpyDeviceToHost, s) != cudaSuccess) return JET_ERR_CUDA;
-    if (cudaStreamSynchronize(s) != cudaSuccess) return JET_ERR_CUDA;
-    if (res[6]) return JET_ERR_INVALID;  // a part id outside [0, k)
+    e = cudaMemcpyAsync(res, scr + 8 + 2 * MAX_PARTS, sizeof(res), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_fail("copying the results", e);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail("stream synchronisation", e);
+    if (res[6]) {
+        set_last_error("jet_pstat_noalloc: a part id lies outside [0, k)");
+        return JET_ERR_INVALID;
+    }
     (void)nnz;
     for (int i = 0; i < 6; i++) out[i] = (int64_t)res[i];
     return JET_OK;
@@ -166,13 +188,21 @@ static int run(int64_t n, int64_t nnz, const void* row, const void* adj, const v
 extern "C" int jet_pstat_noalloc(int tier, int64_t n, int64_t nnz, const void* row_map, const void* entries, const void* values,
                                  const void* vweights, const int32_t* part, int32_t k, int64_t* out, void* stream) {
     using namespace jetb::noalloc;
-    if (!out || n < 0 || (n > 0 && (!row_map || !part || !vweights))) return JET_ERR_INVALID;
-    if (k < 1 || k > MAX_PARTS) return JET_ERR_INVALID;  // the scratch array serves at most MAX_PARTS parts
+    if (!out || n < 0 || nnz < 0 || (n > 0 && (!row_map || !part || !vweights)) || (nnz > 0 && (!entries || !values))) {
+        jetb::set_last_error("jet_pstat_noalloc: null array or negative size");
+        return JET_ERR_INVALID;
+    }
+    if (k < 1 || k > MAX_PARTS) {  // the scratch array serves at most MAX_PARTS parts
+        jetb::set_last_error("jet_pstat_noalloc: num_parts must lie in [1, 16384]");
+        return JET_ERR_INVALID;
+    }
     cudaStream_t s = (cudaStream_t)stream;  // NULL: the legacy default stream
     switch (tier) {
         case 0: return run<int32_t, int32_t, int32_t>(n, nnz, row_map, entries, values, vweights, part, k, out, s);
         case 1: return run<int32_t, int64_t, int64_t>(n, nnz, row_map, entries, values, vweights, part, k, out, s);
         case 2: return run<int64_t, int64_t, int64_t>(n, nnz, row_map, entries, values, vweights, part, k, out, s);
-        default: return JET_ERR_INVALID;
+        default:
+            jetb::set_last_error("jet_pstat_noalloc: tier must be 0, 1 or 2");
+            return JET_ERR_INVALID;
     }
 }

@@ -106,6 +106,12 @@ def _gen(seed: int, device) -> torch.Generator:
     return g
 
 
+def _randint_cpu(lo: int, hi: int, count: int, seed: int, device) -> torch.Tensor:
+    """Integers uniform in [lo, hi) drawn on the host from ``seed``, so that a
+    graph is the same whichever device it is built on."""
+    return torch.randint(lo, hi, (count,), generator=_gen(seed, "cpu")).to(device)
+
+
 def grid2d(nx: int, ny: int, weighted: bool = False, seed: int = 1, tier: str = "i32", device="cpu") -> CSRGraph:
     idx = torch.arange(nx * ny, device=device).reshape(ny, nx)
     us = [idx[:, :-1].reshape(-1), idx[:-1, :].reshape(-1)]
@@ -114,19 +120,20 @@ def grid2d(nx: int, ny: int, weighted: bool = False, seed: int = 1, tier: str = 
     v = torch.cat(vs)
     w = None
     if weighted:
-        w = torch.randint(1, 11, (u.numel(),), generator=_gen(seed, device), device=device)
+        w = _randint_cpu(1, 11, u.numel(), seed, device)
     return from_undirected(nx * ny, u, v, w, tier)
 
 
 def grid3d(nx: int, ny: int, nz: int, weighted: bool = True, seed: int = 1, tier: str = "i32", device="cpu") -> CSRGraph:
     """7-point 3D grid; with ``weighted`` each undirected edge gets a weight
-    uniform in [1, 10] drawn from ``seed``."""
+    uniform in [1, 10] drawn from ``seed`` (on the host: the same graph on
+    every device)."""
     idx = torch.arange(nx * ny * nz, device=device).reshape(nz, ny, nx)
     u = torch.cat([idx[:, :, :-1].reshape(-1), idx[:, :-1, :].reshape(-1), idx[:-1, :, :].reshape(-1)])
     v = torch.cat([idx[:, :, 1:].reshape(-1), idx[:, 1:, :].reshape(-1), idx[1:, :, :].reshape(-1)])
     w = None
     if weighted:
-        w = torch.randint(1, 11, (u.numel(),), generator=_gen(seed, device), device=device)
+        w = _randint_cpu(1, 11, u.numel(), seed, device)
     return from_undirected(nx * ny * nz, u, v, w, tier)
 
 
@@ -164,8 +171,8 @@ def rgg(n: int, mean_degree: float = 10.0, seed: int = 1, weighted: bool = True,
     """Random geometric graph: n points uniform in the unit square, an edge
     between points closer than r = sqrt(mean_degree / (pi n)); weights uniform
     in [1, 10] when ``weighted``."""
-    gen = _gen(seed, device)
-    pts = torch.rand(n, 2, generator=gen, device=device, dtype=torch.float64)
+    gen = _gen(seed, "cpu")
+    pts = torch.rand(n, 2, generator=gen, dtype=torch.float64).to(device)
     r = math.sqrt(mean_degree / (math.pi * n))
     cells = max(1, int(1.0 / r))
     cx = (pts[:, 0] * cells).long().clamp_(max=cells - 1)
@@ -202,7 +209,7 @@ def rgg(n: int, mean_degree: float = 10.0, seed: int = 1, weighted: bool = True,
     v = torch.cat(vs)
     w = None
     if weighted:
-        w = torch.randint(1, 11, (u.numel(),), generator=gen, device=device)
+        w = torch.randint(1, 11, (u.numel(),), generator=gen).to(device)
     return from_undirected(n, u, v, w, tier)
 
 

@@ -65,3 +65,14 @@ def table_multisets(off, ent, val, size):
         keep = e >= 0
         out.append(sorted(zip(e[keep].tolist(), v[keep].tolist())))
     return out
+
+
+@pytest.fixture(scope="session")
+def ref():
+    """The reference's own CPU code (oracle/_ref); tests using it skip when it
+    is neither built nor buildable here."""
+    import ref as ref_mod
+    if not ref_mod.available():
+        pytest.skip("reference build unavailable")
+    ref_mod.lib()
+    return ref_mod
