@@ -7,8 +7,11 @@
 // light structs over raw pointers -- device pointers for the default-space
 // types (matrix_t, wgt_vt, part_vt), host pointers for the *_host / *_serial
 // types -- exposing the members the reference's callers use (numRows(),
-// nnz(), graph.row_map, graph.entries, values).  All computation runs on the
-// current CUDA device either way.  Errors throw jet_partitioner::jet_error
+// nnz(), graph.row_map, graph.entries, values), the allocating
+// View("label", n) constructor, deep_copy and create_mirror_view_and_copy.
+// Device-space partition calls return an owning device view, host-space ones
+// an owning host view.  All computation runs on the current CUDA device
+// either way.  Errors throw jet_partitioner::jet_error
 // (the reference exits on a Metis failure, src/initial_partition.hpp:106-109).
 #pragma once
 
@@ -53,19 +56,72 @@ struct jet_error : std::runtime_error {
 
 enum class Space { Device, Host };
 
-// A one-dimensional view: pointer + extent (+ owning storage for results).
+// A one-dimensional view: pointer + extent, optionally owning its storage.
+//   View(ptr, n)        wraps caller memory (host or device, by S);
+//   View("label", n)    allocates n zeroed elements and owns them, as
+//                       Kokkos::View("label", n) does (app/driver.cpp:102):
+//                       host memory for Space::Host, device memory of the
+//                       current CUDA device for Space::Device.
+// Copies share storage (reference counted), as Kokkos views do.
 template <class T, Space S>
 struct View {
+    using value_type = T;
+    using HostMirror = View<T, Space::Host>;
     T* ptr = nullptr;
     size_t n = 0;
-    std::shared_ptr<std::vector<T>> host_store;  // owner of host results
+    std::shared_ptr<void> owner;
     View() {}
     View(T* p, size_t count) : ptr(p), n(count) {}
+    View(const std::string& label, size_t count) : n(count) {
+        (void)label;
+        if (S == Space::Host) {
+            auto store = std::make_shared<std::vector<T>>(count, T());
+            ptr = store->data();
+            owner = store;
+        } else {
+            void* p = nullptr;
+            int rc = jet_device_alloc((int64_t)(count * sizeof(T)), &p);
+            if (rc != JET_OK) throw std::runtime_error(std::string("jet: device allocation failed: ") + jet_last_error());
+            owner = std::shared_ptr<void>(p, [](void* q) { jet_device_free(q); });
+            ptr = static_cast<T*>(p);
+            if (count) {
+                std::vector<T> zeros(count, T());
+                jet_copy(ptr, zeros.data(), (int64_t)(count * sizeof(T)));
+            }
+        }
+    }
+    View(const char* label, size_t count) : View(std::string(label), count) {}
     T* data() const { return ptr; }
     size_t extent(int) const { return n; }
     size_t size() const { return n; }
     T& operator()(size_t i) const { return ptr[i]; }  // host views only
 };
+
+// Kokkos::deep_copy counterparts for these views: fill with a value, or copy
+// between any two views of equal extent (host or device, either direction).
+template <class T, Space S, class U>
+void deep_copy(const View<T, S>& dst, const U& value) {
+    if (S == Space::Host) {
+        for (size_t i = 0; i < dst.n; i++) dst.ptr[i] = (T)value;
+    } else if (dst.n) {
+        std::vector<T> tmp(dst.n, (T)value);
+        if (jet_copy(dst.ptr, tmp.data(), (int64_t)(dst.n * sizeof(T))) != JET_OK)
+            throw std::runtime_error(std::string("jet: deep_copy failed: ") + jet_last_error());
+    }
+}
+template <class T, Space S1, Space S2>
+void deep_copy(const View<T, S1>& dst, const View<T, S2>& src) {
+    if (dst.n != src.n) throw std::runtime_error("jet: deep_copy between views of different extents");
+    if (dst.n && jet_copy(dst.ptr, src.ptr, (int64_t)(dst.n * sizeof(T))) != JET_OK)
+        throw std::runtime_error(std::string("jet: deep_copy failed: ") + jet_last_error());
+}
+// Kokkos::create_mirror_view_and_copy: a host copy of any view.
+template <class T, Space S>
+View<T, Space::Host> create_mirror_view_and_copy(const View<T, S>& v) {
+    View<T, Space::Host> h("mirror", v.n);
+    deep_copy(h, v);
+    return h;
+}
 
 // KokkosSparse::CrsMatrix shape (header/jet_defs.h:64-92).
 template <class Val, class Ord, class Off, Space S>
@@ -100,7 +156,7 @@ using wgt_serial_vt = wgt_host_vt;
 using big_wgt_vt = View<big_val_t, Space::Device>;
 using big_wgt_host_vt = View<big_val_t, Space::Host>;
 using big_wgt_serial_vt = big_wgt_host_vt;
-using part_vt = View<part_t, Space::Device>;  // caller provides the device buffer via set_output()
+using part_vt = View<part_t, Space::Device>;  // device partitions come back in library-allocated, owning views
 using part_mt = View<part_t, Space::Host>;
 
 // header/experiment_data.hpp:50-72
@@ -175,43 +231,33 @@ inline jet_config_c to_c(const config_t& c) {
 inline void check(int rc) {
     if (rc != JET_OK) throw jet_error(rc, std::string("jet: ") + jet_last_error());
 }
-// Device results need a device buffer: the caller passes one through
-// set_device_output() before calling, as Kokkos would have allocated it.
-inline part_t*& device_out() {
-    static thread_local part_t* p = nullptr;
-    return p;
-}
 inline uint64_t& seed() {
     static thread_local uint64_t s = 1;
     return s;
 }
 }  // namespace detail
 
-// Device buffer of numRows() ints that the next device-space partition call fills.
-inline void set_device_output(part_t* dev_ptr) { detail::device_out() = dev_ptr; }
 // Coarsening RNG seed (the reference seeds from the clock, src/contract.hpp:503).
 inline void set_seed(uint64_t s) { detail::seed() = s; }
 
+// Device-space calls return a fresh device view the caller owns, as the
+// reference returns a freshly allocated Kokkos view (header/jet.h:46-51).
 template <class Mat, class WV, class Cut, class Fn>
 part_vt partition_device_impl(Cut& edge_cut, const config_t& config, const Mat& g, const WV& vweights, bool uniform_ew,
                               experiment_data<Cut>& experiment, Fn fn) {
-    part_t* out = detail::device_out();
-    if (!out) throw jet_error(JET_ERR_INVALID, "jet: call set_device_output() with a device buffer first");
+    part_vt out("part", (size_t)g.numRows());
     jet_config_c c = detail::to_c(config);
     jet_stats_c st;
     detail::check(fn(&c, g.numRows(), g.graph.row_map.data(), g.graph.entries.data(), g.values.data(), vweights.data(),
-                     (int)uniform_ew, JET_MEM_DEVICE, detail::seed(), nullptr, out, &edge_cut, &st));
+                     (int)uniform_ew, JET_MEM_DEVICE, detail::seed(), nullptr, out.data(), &edge_cut, &st));
     experiment.fill(st);
-    return part_vt(out, (size_t)g.numRows());
+    return out;
 }
 
 template <class Mat, class WV, class Cut, class Fn>
 part_mt partition_host_impl(Cut& edge_cut, const config_t& config, const Mat& g, const WV& vweights, bool uniform_ew,
                             experiment_data<Cut>& experiment, Fn fn) {
-    part_mt res;
-    res.host_store = std::make_shared<std::vector<part_t>>((size_t)g.numRows());
-    res.ptr = res.host_store->data();
-    res.n = (size_t)g.numRows();
+    part_mt res("part", (size_t)g.numRows());
     jet_config_c c = detail::to_c(config);
     jet_stats_c st;
     detail::check(fn(&c, g.numRows(), g.graph.row_map.data(), g.graph.entries.data(), g.values.data(), vweights.data(),

@@ -45,7 +45,7 @@ typedef struct jet_config_c {
     double max_imb_ratio;
     int32_t num_parts;
     double refine_tolerance;  /* default 0.999 */
-    int32_t dump_coarse;      /* accepted, ignored (experiment dump) */
+    int32_t dump_coarse;      /* write coarse_graphs.out / coarse_part.out (src/binary_dump.hpp) */
     int32_t verbose;
     int32_t ultra_settings;
 } jet_config_c;
@@ -255,15 +255,55 @@ const char* jet_last_error(void);
 int jet_device_ok(void);
 
 /* Kernel-class timing with CUDA events on the launching stream (used by the
- * benchmark).  kinds: 0 conn build, 1 LP select, 2 afterburner, 3 table
- * updates, 4 contraction, 5 heavy-edge proposal, 6 conn build of the finest
- * level only.  jet_prof_read fills ms[7], bytes[7] (algorithmic bytes),
- * launches[7]. */
+ * benchmark).  Classes: 0 table build, 1 LP select, 2 afterburner, 3 small
+ * table update, 4 contraction (phase, host syncs included), 5 coarsening map
+ * (phase), 6 table build of the finest level only, 7 rebalance select/score,
+ * 8 rebalance sort, 9 eviction, 10 apply moves, 11 large table update,
+ * 12 cut change.  Classes 1-3 and 7-12 are bracketed on levels that run on
+ * the host-driven loop (set jet_set_refine_drivers(0) to run every level
+ * there); their algorithmic bytes come from device-side counts of that
+ * iteration.  jet_prof_read fills ms[13], bytes[13], launches[13]. */
 int jet_prof_enable(int on);
 int jet_prof_read(double* ms, double* bytes, int64_t* launches);
 
 /* Number of CUDA kernels this library has launched in this process. */
 int64_t jet_launch_count(void);
+
+/* Test hooks for failure handling (no counterpart in the reference, whose
+ * only failure path, a Metis error, exits the process:
+ * src/initial_partition.hpp:106-109).  None faults, traps or hangs a GPU.
+ *   jet_test_inject_metis_failures(count): the next `count` Metis calls of
+ *     this process report METIS_ERROR without running (the partition call
+ *     then returns JET_ERR_METIS); returns the previous count.
+ *   jet_test_grid_barrier: one cooperative launch of `blocks` blocks that
+ *     meet `rounds` times at the cooperative level driver's software grid
+ *     barrier, each wait limited to 2^spin_cap_log2 polls; absent_block
+ *     (or -1) never arrives.  JET_OK when every barrier completed,
+ *     JET_ERR_TIMEOUT when a wait ran out; *passed = barrier passages.
+ *   jet_test_table_overflow: inserts parts 0..nparts-1 into a shared-memory
+ *     connectivity table of `cap` slots (k parts) with the table-build insert;
+ *     JET_ERR_OVERFLOW when the probe bound flagged a full table. */
+int jet_test_inject_metis_failures(int count);
+int jet_test_grid_barrier(int blocks, int absent_block, int spin_cap_log2, int rounds, int* passed);
+int jet_test_table_overflow(int cap, int k, int nparts, int* claimed);
+
+/* Device memory for callers without a CUDA toolchain of their own (the C++
+ * drop-in include/jet.h uses these for the device views it allocates, as
+ * Kokkos allocates the reference's View("label", n), app/driver.cpp:102).
+ * jet_copy copies between any two host or device pointers (cudaMemcpyDefault). */
+int jet_device_alloc(int64_t bytes, void** ptr);
+
+/* METIS text graph reader with the reference's rules (app/io.hpp:99-217),
+ * parsed in parallel on `threads` host threads (0 = all cores).  Allocates
+ * row_map[n+1], entries[nnz] and values[nnz] in host memory in the tier's
+ * integer types; release each with jet_free_host.  Unweighted files (fmt 0)
+ * give unit edge weights and *uniform_ew = 1.  JET_ERR_INVALID on a
+ * malformed file (message in jet_last_error()). */
+int jet_read_metis(const char* path, int tier, int threads, int64_t* n, int64_t* nnz, void** row_map, void** entries,
+                   void** values, int* uniform_ew);
+void jet_free_host(void* ptr);
+int jet_device_free(void* ptr);
+int jet_copy(void* dst, const void* src, int64_t bytes);
 
 /* Level-loop drivers refinement may use, process-wide (no counterpart in the
  * reference, whose loop is always host-driven, src/jet_refiner.hpp:1094-1134).

@@ -57,6 +57,8 @@ EXPORTED_SYMBOLS = [
     "jet_last_error", "jet_device_ok", "jet_prof_enable", "jet_prof_read", "jet_launch_count", "jet_pstat_noalloc",
     "jet_set_refine_drivers", "jet_partition_batch", "jet_server_create", "jet_server_submit", "jet_server_wait",
     "jet_server_footprint", "jet_server_stats_get", "jet_server_destroy", "jet_refine_hierarchy",
+    "jet_device_alloc", "jet_device_free", "jet_copy", "jet_read_metis", "jet_free_host",
+    "jet_test_inject_metis_failures", "jet_test_grid_barrier", "jet_test_table_overflow",
 ]
 
 # level-loop drivers (jet_set_refine_drivers)
@@ -636,10 +638,16 @@ def prof_enable(on: bool = True):
     _check(load().jet_prof_enable(int(on)))
 
 
+PROF_CLASSES = ["conn_build", "lp_select", "afterburn", "update", "contract", "coarsen_map", "conn_build_finest",
+                "reb_select", "reb_sort", "reb_evict", "apply", "update_large", "cut_after"]
+
+
 def prof_read():
-    ms = (ctypes.c_double * 7)()
-    by = (ctypes.c_double * 7)()
-    ln = (ctypes.c_int64 * 7)()
+    """Per kernel class: summed event time (ms), algorithmic bytes, launches."""
+    nk = len(PROF_CLASSES)
+    ms = (ctypes.c_double * nk)()
+    by = (ctypes.c_double * nk)()
+    ln = (ctypes.c_int64 * nk)()
     _check(load().jet_prof_read(ms, by, ln))
-    names = ["conn_build", "lp_select", "afterburn", "update", "contract", "coarsen_map", "conn_build_finest"]
+    names = PROF_CLASSES
     return {nm: dict(ms=ms[i], bytes=by[i], launches=ln[i]) for i, nm in enumerate(names)}

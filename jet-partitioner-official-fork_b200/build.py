@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libjetb200.so")
 HELPER = os.path.join(HERE, "jet_metis_helper")
 BUILD = os.path.join(HERE, "_build")
-UNITS = ["runtime.cu", "tier_i32.cu", "tier_big.cu", "tier_biggest.cu", "noalloc.cu", "batch.cu"]
+UNITS = ["runtime.cu", "tier_i32.cu", "tier_big.cu", "tier_biggest.cu", "noalloc.cu", "batch.cu", "metis_io.cpp", "test_hooks.cu"]
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 METIS = os.path.join(CUDA, "targets", "x86_64-linux", "lib", "libmetis_static.a")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -43,7 +43,7 @@ def build(force: bool = False, ptxas_verbose: bool = False) -> str:
     extra = ["-Xptxas", "-v"] if ptxas_verbose else []
 
     def compile_unit(u):
-        obj = os.path.join(BUILD, u.replace(".cu", ".o"))
+        obj = os.path.join(BUILD, os.path.splitext(u)[0] + ".o")
         cmd = ["nvcc", *NVCC_FLAGS, *extra, "-c", os.path.join(CSRC, u), "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         return u, obj, r

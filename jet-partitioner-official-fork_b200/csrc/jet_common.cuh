@@ -441,15 +441,25 @@ enum ProfKernel : int {
     PK_CONN_BUILD = 0,
     PK_LP_SELECT,
     PK_AFTERBURN,
-    PK_UPDATE,
+    PK_UPDATE,       // update_small (both passes)
     PK_CONTRACT,
     PK_HEC,
     PK_CONN_FINEST,  // the table build of the finest level alone
+    PK_REB_SELECT,   // weak destination select / strong eviction scores
+    PK_REB_SORT,     // bucket offsets, candidate sort, weight prefix
+    PK_REB_EVICT,    // eviction filter (+ strong: cookie cutter, draws)
+    PK_APPLY,        // apply moves and part sizes
+    PK_UPDATE_LARGE, // update_large: mark neighbours, rebuild their rows
+    PK_CUT_AFTER,    // cut change part 2
     PK_COUNT
 };
-// Marks the start/end of a timed launch group.  bytes = algorithmic bytes.
+// Marks the start/end of a timed launch group.  bytes = algorithmic bytes;
+// prof_add_bytes adds to a group already ended (counts known only after the
+// iteration's sync).
 int prof_begin(cudaStream_t s);
 void prof_end(int h, ProfKernel k, double bytes, cudaStream_t s);
+void prof_add_bytes(int h, double bytes);
+bool prof_active();
 void prof_collect();  // after a stream sync: folds event pairs into the slots
 
 }  // namespace jetb

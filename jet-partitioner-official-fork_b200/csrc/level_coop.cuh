@@ -25,7 +25,8 @@ struct GridBar {
 };
 
 // Returns false when the loop must stop (a barrier timed out somewhere).
-__device__ __forceinline__ bool grid_sync(GridBar* gb, int* err) {
+// A wait gives up after spin_cap polls (2^26, about 4 s, by default).
+__device__ __forceinline__ bool grid_sync(GridBar* gb, int* err, long long spin_cap = (1ll << 26)) {
     __syncthreads();
     if (threadIdx.x == 0) {
         volatile unsigned int* vgen = &gb->gen;
@@ -40,7 +41,7 @@ __device__ __forceinline__ bool grid_sync(GridBar* gb, int* err) {
             long long spins = 0;
             while (*vgen == g) {
                 if (((volatile int*)&gb->abort)[0]) break;
-                if (++spins > (1ll << 26)) {
+                if (++spins > spin_cap) {
                     atomicOr(err, ERRF_SPIN);
                     atomicExch(&gb->abort, 1);
                     break;

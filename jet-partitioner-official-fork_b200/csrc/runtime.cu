@@ -275,8 +275,14 @@ void release_helper(int i, bool ok) {
 }
 }  // namespace
 
+// Failures injected by jet_test_inject_metis_failures: the next calls
+// report METIS_ERROR without running Metis.
+static std::atomic<int> g_metis_fail{0};
+
 int metis_kway(int64_t n, int64_t m, int64_t* xadj, int64_t* adj, int64_t* vw, int64_t* ew, int64_t nparts, float ub,
                int64_t* obj, int64_t* part) {
+    for (int f = g_metis_fail.load(); f > 0; f = g_metis_fail.load())
+        if (g_metis_fail.compare_exchange_weak(f, f - 1)) return -4;  // METIS_ERROR
     if (t_batch) {
         int fd = -1;
         int hi = acquire_helper(&fd);
@@ -386,6 +392,18 @@ int prof_begin(cudaStream_t s) {
     return h;
 }
 
+bool prof_active() {
+    std::lock_guard<std::recursive_mutex> lk(g_prof_mu);
+    return g_prof.on && !capturing();
+}
+
+void prof_add_bytes(int h, double bytes) {
+    std::lock_guard<std::recursive_mutex> lk(g_prof_mu);
+    if (h < 0 || !g_prof.on) return;
+    for (auto it = g_prof.pending.rbegin(); it != g_prof.pending.rend(); ++it)
+        if (it->ev == h) { it->bytes += bytes; return; }
+}
+
 void prof_end(int h, ProfKernel k, double bytes, cudaStream_t s) {
     std::lock_guard<std::recursive_mutex> lk(g_prof_mu);
     if (h < 0 || !g_prof.on || capturing()) return;
@@ -491,6 +509,41 @@ int jet_project(int tier, int64_t n_fine, const void* map, const int32_t* coarse
 }
 
 int64_t jet_launch_count(void) { return g_launches.load(); }
+
+int jet_test_inject_metis_failures(int count) { return g_metis_fail.exchange(count < 0 ? 0 : count); }
+
+int jet_device_alloc(int64_t bytes, void** ptr) {
+    if (!ptr || bytes < 0) return JET_ERR_INVALID;
+    *ptr = nullptr;
+    if (bytes == 0) return JET_OK;
+    cudaError_t e = cudaMalloc(ptr, (size_t)bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        g_last_error = std::string("jet_device_alloc: ") + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? JET_ERR_OOM : JET_ERR_CUDA;
+    }
+    return JET_OK;
+}
+
+int jet_device_free(void* ptr) {
+    if (ptr && cudaFree(ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return JET_ERR_CUDA;
+    }
+    return JET_OK;
+}
+
+int jet_copy(void* dst, const void* src, int64_t bytes) {
+    if (bytes < 0 || (bytes > 0 && (!dst || !src))) return JET_ERR_INVALID;
+    if (bytes == 0) return JET_OK;
+    cudaError_t e = cudaMemcpy(dst, src, (size_t)bytes, cudaMemcpyDefault);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        g_last_error = std::string("jet_copy: ") + cudaGetErrorString(e);
+        return JET_ERR_CUDA;
+    }
+    return JET_OK;
+}
 
 int jet_set_refine_drivers(int mask) { return g_drivers.exchange(mask & JET_DRIVER_ALL); }
 

@@ -5,6 +5,7 @@
 #include "partitioner.cuh"
 #include "sort.cuh"
 #include "level_coop.cuh"
+#include "prof.cuh"
 
 namespace jetb {
 
@@ -92,6 +93,8 @@ struct Refiner {
         dev.zero();
         ctl.alloc(1, s);
         ctl.zero();
+        pcount.alloc(1, s);
+        ph_reset();
         int drv = refine_drivers();
         use_cta = (drv & JET_DRIVER_CTA) != 0;
         use_coop = (drv & JET_DRIVER_COOP) != 0;
@@ -271,9 +274,16 @@ struct Refiner {
         return (int64_t)C;
     }
 
+    // Profiling-pass handles of the current iteration's class brackets.
+    int ph[PK_COUNT];
+    int ph_mark = -1;
+    DBuf<ProfCounts> pcount;
+    void ph_reset() { for (int i = 0; i < PK_COUNT; i++) ph[i] = -1; ph_mark = -1; }
+
     void lp(const Level<O, E, W>& L) {
         auto a = args(L);
         int h = prof_begin(s);
+        ph[PK_LP_SELECT] = h;
         k_lp_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a); count_launch();
         JET_LAUNCH_CHECK();
         if (L.n_warp > 0) { k_lp_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, L.warp_list.p, L.n_warp); count_launch(); }
@@ -281,6 +291,7 @@ struct Refiner {
         JET_LAUNCH_CHECK();
         prof_end(h, PK_LP_SELECT, 0, s);
         h = prof_begin(s);
+        ph[PK_AFTERBURN] = h;
         unsigned grid = grid_persistent((int64_t)L.n * L.group, 16);
         switch (L.group) {
             case 4: k_afterburn<4, O, E, W><<<grid, BLOCK, 0, s>>>(a); count_launch(); break;
@@ -339,32 +350,53 @@ struct Refiner {
     void weak(const Level<O, E, W>& L, W opt, W size_max) {
         auto a = args(L);
         auto rb = reb_args(L, weak_max_dest(size_max), opt, size_max);
+        int h = ph[PK_REB_SELECT] = prof_begin(s);
         k_weak_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
         k_weak_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
         if (L.n_warp > 0) { k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp); count_launch(); }
         if (L.n_hub > 0) { k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub); count_launch(); }
         JET_LAUNCH_CHECK();
+        prof_end(h, PK_REB_SELECT, 0, s);
+        h = ph[PK_REB_SORT] = prof_begin(s);
         sort_candidates(L, rb);
+        prof_end(h, PK_REB_SORT, reb_sort_bytes(L, rb), s);
+        h = ph[PK_REB_EVICT] = prof_begin(s);
         k_evict_sorted<false, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
         JET_LAUNCH_CHECK();
+        prof_end(h, PK_REB_EVICT, 0, s);
+    }
+
+    // Algorithmic bytes of sort_candidates: the bucket scan, each radix pass
+    // reading and writing (key, vertex) pairs, and the weight prefix.
+    double reb_sort_bytes(const Level<O, E, W>& L, const RebArgs<O, W>& rb) const {
+        const double n = (double)L.n;
+        const int passes = (bits_for((uint64_t)rb.none_key) + 7) / 8;
+        return 2.0 * ((double)rb.t_minibuckets + 1) * sizeof(W) + passes * n * 2.0 * (4 + sizeof(O)) +
+               n * (4 + sizeof(O) + 2 * sizeof(W));
     }
 
     // rebalance_strong, src/jet_refiner.hpp:417-546.
     void strong(const Level<O, E, W>& L, W opt, W size_max) {
         auto a = args(L);
         auto rb = reb_args(L, strong_max_dest(opt, size_max), opt, size_max);
+        int h = ph[PK_REB_SELECT] = prof_begin(s);
         k_strong_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
         k_strong_score_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
         if (L.n_warp > 0) { k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_warp * 32, 16), BLOCK, 0, s>>>(a, rb, L.warp_list.p, L.n_warp); count_launch(); }
         if (L.n_hub > 0) { k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub); count_launch(); }
         JET_LAUNCH_CHECK();
+        prof_end(h, PK_REB_SELECT, 0, s);
+        h = ph[PK_REB_SORT] = prof_begin(s);
         sort_candidates(L, rb);
+        prof_end(h, PK_REB_SORT, reb_sort_bytes(L, rb), s);
+        h = ph[PK_REB_EVICT] = prof_begin(s);
         JET_CUDA(cudaMemsetAsync(evict_adjust.p, 0, sizeof(W) * k, s));
         k_evict_sorted<true, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
         k_cookie<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
         k_strong_first<O, E, W><<<grid_persistent(L.n, 8), BLOCK, 0, s>>>(a, rb); count_launch();
         k_strong_redraw<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
         JET_LAUNCH_CHECK();
+        prof_end(h, PK_REB_EVICT, 0, s);
     }
 
     // perform_moves, src/jet_refiner.hpp:905-955, in four parts: the moves
@@ -414,6 +446,13 @@ struct Refiner {
         count_launch();
         if (L.n_hub > 0) { k_mark_neighbors_hub<O, E, W><<<device_info().sms * 2, 1024, 0, s>>>(a); count_launch(); }
         JET_LAUNCH_CHECK();
+        if (ph_mark >= 0) {
+            // profiling pass: count the marked rows between the two brackets
+            prof_end(ph_mark, PK_UPDATE_LARGE, 0, s);
+            k_prof_marked<O, E, W><<<grid_persistent(L.n, 4), BLOCK, 0, s>>>(a, pcount.p); count_launch();
+            JET_LAUNCH_CHECK();
+            ph[PK_UPDATE_LARGE] = prof_begin(s);
+        }
         build_tables(L, 1, &dev.p->large);
     }
     void cut_after_kernel(const Level<O, E, W>& L) {
@@ -421,17 +460,79 @@ struct Refiner {
         JET_LAUNCH_CHECK();
     }
     void moves_kernels(const Level<O, E, W>& L) {
+        ph[PK_UPDATE_LARGE] = -1;
+        int h = ph[PK_APPLY] = prof_begin(s);
         apply_moves_kernel(L);
-        int h = prof_begin(s);
+        prof_end(h, PK_APPLY, 0, s);
+        h = ph[PK_UPDATE] = prof_begin(s);
         small_update_kernels(L);
-        large_update_kernels(L);
         prof_end(h, PK_UPDATE, 0, s);
+        ph_mark = prof_begin(s);
+        large_update_kernels(L);
+        if (ph[PK_UPDATE_LARGE] >= 0) prof_end(ph[PK_UPDATE_LARGE], PK_UPDATE_LARGE, 0, s);
+        h = ph[PK_CUT_AFTER] = prof_begin(s);
         cut_after_kernel(L);
+        prof_end(h, PK_CUT_AFTER, 0, s);
+    }
+
+    // Profiling pass, after an iteration's sync: the device counts turned
+    // into each class bracket's algorithmic bytes (each array element counted
+    // once per bracket: reads of what the class must read, writes of what it
+    // produces; a table probe counts one slot).
+    void prof_account(const Level<O, E, W>& L, int kind, const IterResult& r) {
+        ProfCounts c;
+        JET_CUDA(cudaMemcpyAsync(e.hscal, pcount.p, sizeof(ProfCounts), cudaMemcpyDeviceToHost, s));
+        e.sync();
+        std::memcpy(&c, e.hscal, sizeof(ProfCounts));
+        const double so = sizeof(O), se = sizeof(E), sw = sizeof(W), sl = sizeof(Slot<W>);
+        const double n = (double)L.n, T = (double)c.moves, Td = (double)c.moves_deg;
+        if (kind == 0) {
+            // LP select: cache test and destination write for every vertex;
+            // the uncached ones read part, offset, size and their table and
+            // write gain and cache; candidates are appended
+            prof_add_bytes(ph[PK_LP_SELECT], n * (4 + 4) + (double)c.uncached * (4 + se + 4 + sw + 4) +
+                                                 (double)c.size_uncached * sl + (double)c.cand * so);
+            // afterburner: each candidate's row, pregain, part and destination;
+            // per edge the neighbour, weight and the neighbour's pregain,
+            // destination and part; the kept ones are locked and appended
+            prof_add_bytes(ph[PK_AFTERBURN], (double)c.cand * (so + 2 * se + sw + 4 + 4) +
+                                                 (double)c.cand_deg * (so + sw + sw + 4 + 4) + T * (1 + so));
+        } else {
+            // weak select / strong scores: every vertex's part, weight, table
+            // offset and size and its whole table; bucket id and score out
+            prof_add_bytes(ph[PK_REB_SELECT], n * (4 + sw + se + 4 + 4 + sw) + (double)c.csize_all * sl);
+            // eviction filter over the sorted candidates; the moves appended
+            prof_add_bytes(ph[PK_REB_EVICT], n * (4 + so + sw + 4) + T * (so + 4));
+        }
+        // apply: per move its vertex, part, destination and weight, the part
+        // and destination writes, the two size updates
+        prof_add_bytes(ph[PK_APPLY], T * (so + 4 + 4 + sw + 4 + 4 + 4) + 2.0 * k * sw);
+        if (r.large) {
+            // mark: each moved vertex's row and its neighbours' marks
+            prof_add_bytes(ph_mark, Td * (so + 1) + T * 2 * se);
+            // rebuild: each marked row, its neighbours' parts and the table
+            prof_add_bytes(ph[PK_UPDATE_LARGE], (double)c.marked * (2 * se + 1 + 4) +
+                                                    (double)c.marked_deg * (so + sw + 4) + (double)c.marked_cap * sl);
+        } else {
+            // small update, subtract then add: per moved edge the neighbour,
+            // weight, the neighbour's table offset, size and one slot
+            // read-modify-write, twice
+            prof_add_bytes(ph[PK_UPDATE], 2.0 * Td * (so + sw + se + 4 + 2 * sl) + T * (so + 2 * se + 8));
+        }
+        // cut change part 2: per move two lookups in its own table
+        prof_add_bytes(ph[PK_CUT_AFTER], T * (so + se + 4 + 8 + 2 * sl));
     }
 
     // Host-driven iteration end: results to pinned memory, one host sync.
     IterResult perform_moves(const Level<O, E, W>& L) {
         moves_kernels(L);
+        if (ph[PK_APPLY] >= 0) {
+            auto a = args(L);
+            k_prof_list<O, E><<<grid_persistent(L.n, 4), BLOCK, 0, s>>>(a.g.row, a.moves, &a.dev->nmoves, &pcount.p->moves,
+                                                                       &pcount.p->moves_deg);
+            count_launch();
+            JET_LAUNCH_CHECK();
+        }
         k_finalize<O, E, W><<<1, 1024, 0, s>>>(args(L), e.hres); count_launch();
         JET_LAUNCH_CHECK();
         e.sync();
@@ -527,10 +628,25 @@ struct Refiner {
     // One iteration body of jet_refine (src/jet_refiner.hpp:1106-1120).
     int iterate(const Level<O, E, W>& L, const Prob& pb, double filter_ratio, int& balance_counter, int& lab_counter) {
         int kind;
+        ph_reset();
+        const bool pf = prof_active();
+        if (pf) {
+            auto a = args(L);
+            JET_CUDA(cudaMemsetAsync(pcount.p, 0, sizeof(ProfCounts), s));
+            k_prof_select<O, E, W><<<grid_persistent(L.n, 4), BLOCK, 0, s>>>(a, pcount.p); count_launch();
+            JET_LAUNCH_CHECK();
+        }
         if (curr.total_imb <= pb.imb_max) {
             hctl->filter = filter_ratio;
             JET_CUDA(cudaMemcpyAsync(&ctl.p->filter, &hctl->filter, sizeof(double), cudaMemcpyHostToDevice, s));
             lp(L);
+            if (pf) {
+                auto a = args(L);
+                k_prof_list<O, E><<<grid_persistent(L.n, 4), BLOCK, 0, s>>>(a.g.row, a.cand, &a.dev->ncand, &pcount.p->cand,
+                                                                           &pcount.p->cand_deg);
+                count_launch();
+                JET_LAUNCH_CHECK();
+            }
             balance_counter = 0;
             lab_counter++;
             kind = 0;
@@ -540,6 +656,7 @@ struct Refiner {
             balance_counter++;
         }
         IterResult r = perform_moves(L);
+        if (pf) prof_account(L, kind, r);
         curr.cut -= (W)r.cut_change;
         W mx = (W)r.max_part;
         curr.total_imb = mx > pb.opt ? mx - pb.opt : 0;

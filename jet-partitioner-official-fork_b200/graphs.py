@@ -227,40 +227,35 @@ def random_graph(n: int, m: int, seed: int = 1, weighted: bool = True, tier: str
 
 
 # ------------------------------------------------------------------ METIS I/O
-def read_metis(path: str, tier: str = "i32") -> CSRGraph:
-    """METIS text graph (app/io.hpp:99-217): '%' comments, header 'n m [fmt
-    [ncon]]', fmt 0 (no weights) or 1 (edge weights), 1-based neighbour ids.
-    Vertex weights are set to 1 as the reference's driver does
-    (app/driver.cpp:102-103)."""
-    with open(path, "rb") as f:
-        text = f.read().decode()
-    lines = [ln for ln in text.split("\n") if not ln.startswith("%")]
-    head = lines[0].split()
-    n, m = int(head[0]), int(head[1])
-    fmt = int(head[2]) if len(head) > 2 else 0
-    ncon = int(head[3]) if len(head) > 3 else 0
-    if fmt not in (0, 1) or ncon != 0:
-        raise ValueError("unsupported METIS format flags %d / ncon %d (vertex weights are not supported)" % (fmt, ncon))
-    has_ew = fmt % 10 == 1
-    rows = lines[1:1 + n]
-    while len(rows) < n:
-        rows.append("")
-    row = np.zeros(n + 1, dtype=np.int64)
-    adj, val = [], []
-    for i, ln in enumerate(rows):
-        toks = [int(t) for t in ln.split()]
-        if has_ew:
-            adj.extend(t - 1 for t in toks[0::2])
-            val.extend(toks[1::2])
-        else:
-            adj.extend(t - 1 for t in toks)
-        row[i + 1] = len(adj)
-    if row[n] != 2 * m:
-        raise ValueError("METIS file holds %d nonzeros, header promises %d" % (row[n], 2 * m))
+def read_metis(path: str, tier: str = "i32", threads: int = 0) -> CSRGraph:
+    """METIS text graph (app/io.hpp:99-217) read by the library's parallel
+    reader (jet_read_metis): '%' comments, header 'n m [fmt [ncon]]', fmt 0
+    (no weights) or 1 (edge weights), 1-based neighbour ids.  Vertex weights
+    are set to 1 as the reference's driver does (app/driver.cpp:102-103);
+    unweighted files give unit edge weights and uniform=True."""
+    import ctypes
+    from . import load, _check
+    lib = load()
+    n = ctypes.c_int64(0)
+    nnz = ctypes.c_int64(0)
+    row, adj, val = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+    uni = ctypes.c_int(0)
+    _check(lib.jet_read_metis(path.encode(), TIER_ID[tier], int(threads), ctypes.byref(n), ctypes.byref(nnz),
+                              ctypes.byref(row), ctypes.byref(adj), ctypes.byref(val), ctypes.byref(uni)))
     o, e, w = TIERS[tier]
-    val_t = torch.tensor(val, dtype=w) if has_ew else torch.ones(len(adj), dtype=w)
-    return CSRGraph(n, torch.from_numpy(row).to(e), torch.tensor(adj, dtype=o), val_t,
-                    torch.ones(n, dtype=w), not has_ew, tier)
+    try:
+        def grab(ptr, count, dt):
+            npdt = torch.empty(0, dtype=dt).numpy().dtype
+            buf = (ctypes.c_char * (count * npdt.itemsize)).from_address(ptr.value) if count else b""
+            return torch.from_numpy(np.frombuffer(buf, dtype=npdt, count=count).copy())
+        nn, mm = int(n.value), int(nnz.value)
+        row_t = grab(row, nn + 1, e)
+        adj_t = grab(adj, mm, o)
+        val_t = grab(val, mm, w)
+    finally:
+        for ptr in (row, adj, val):
+            lib.jet_free_host(ptr)
+    return CSRGraph(nn, row_t, adj_t, val_t, torch.ones(nn, dtype=w), bool(uni.value), tier)
 
 
 def write_metis(g: CSRGraph, path: str) -> None:

@@ -185,5 +185,23 @@ def gain_bucket(gain: int, vwgt: int, wide: bool = False) -> int:
     return lib().ref_gain_bucket32(ctypes.c_int32(gain), ctypes.c_int32(vwgt))
 
 
+def load_metis(path: str, cap_rows: int, cap_nnz: int):
+    """The reference's own METIS reader (app/io.hpp:99-217), std tier.
+    Returns (row, adj, val, uniform) or None when it rejects the file."""
+    n = ctypes.c_int64(0)
+    nnz = ctypes.c_int64(0)
+    row = np.zeros(cap_rows + 1, dtype=np.int32)
+    adj = np.zeros(max(cap_nnz, 1), dtype=np.int32)
+    val = np.zeros(max(cap_nnz, 1), dtype=np.int32)
+    uni = ctypes.c_int(0)
+    rc = lib().ref_load_metis(path.encode(), ctypes.byref(n), ctypes.byref(nnz), _p(row), ctypes.c_int64(cap_rows + 1),
+                              _p(adj), _p(val), ctypes.c_int64(cap_nnz), ctypes.byref(uni))
+    if rc == 1:
+        return None
+    assert rc == 0, "capacity too small"
+    nn, mm = int(n.value), int(nnz.value)
+    return row[:nn + 1].copy(), adj[:mm].copy(), val[:mm].copy(), bool(uni.value)
+
+
 def pod_hash32(x: int) -> int:
     return int(lib().ref_pod_hash32(ctypes.c_int32(x)))

@@ -29,6 +29,7 @@
 #include "jet_defs.h"
 #include "jet.h"
 #include "partitioner.hpp"
+#include "io.hpp"
 
 using namespace jet_partitioner;
 
@@ -390,6 +391,30 @@ int ref_gain_bucket32(int32_t gain, int32_t vwgt) {
 }
 int ref_gain_bucket64(int64_t gain, int64_t vwgt) {
     return jet_refiner<Mat<int32_t, int64_t, int64_t>, part_t>::gain_bucket(gain, vwgt);
+}
+
+// The reference's own METIS reader (app/io.hpp:99-217), std tier.  Returns
+// 0 and fills n, nnz and the arrays (capacity given by the caller: row_cap
+// entries of row, nnz_cap of adj and val), or 1 when the reader rejects the
+// file, or 2 when the capacity is too small.
+int ref_load_metis(const char* path, int64_t* n, int64_t* nnz, int32_t* row, int64_t row_cap, int32_t* adj,
+                   int32_t* val, int64_t nnz_cap, int* uniform_ew) {
+    matrix_t g;
+    bool uni = false;
+    bool ok;
+    {
+        Quiet q(true);
+        ok = load_metis_graph(g, uni, path);
+    }
+    if (!ok) return 1;
+    *n = g.numRows();
+    *nnz = g.nnz();
+    if (*n + 1 > row_cap || *nnz > nnz_cap) return 2;
+    std::memcpy(row, g.graph.row_map.data(), (size_t)(*n + 1) * sizeof(int32_t));
+    std::memcpy(adj, g.graph.entries.data(), (size_t)*nnz * sizeof(int32_t));
+    std::memcpy(val, g.values.data(), (size_t)*nnz * sizeof(int32_t));
+    *uniform_ew = uni ? 1 : 0;
+    return 0;
 }
 
 // Kokkos::pod_hash of an int32 as the stand-in computes it.
