@@ -127,6 +127,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+_T0 = time.time()
+
+
+def stage(msg):
+    """Progress of the benchmark's legs, to stderr (the JSON line goes to stdout)."""
+    sys.stderr.write("[bench %7.1fs] %s\n" % (time.time() - _T0, msg))
+    sys.stderr.flush()
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -214,7 +223,10 @@ def _batch_ref_one(i):
     k = int(np.load(os.path.join(d, "%d_k.npy" % i)))
     og = oracle.G(*arr, uniform=False)
     t = time.perf_counter()
-    _, cut, _, _ = ref.partition(og, k, alg=1, imb=1.03, seed=i + 1, space="serial")
+    try:
+        _, cut, _, _ = ref.partition(og, k, alg=1, imb=1.03, seed=i + 1, space="serial")
+    except ref.ReferenceCrash:
+        cut = None  # the reference divided by zero on this graph (no undersized part in rebalance_weak)
     return time.perf_counter() - t, cut
 
 
@@ -233,15 +245,22 @@ def run_batched_cpu(gs, cfgs, cores):
             np.save(os.path.join(tmp, "%d_k.npy" % i), np.int64(c.num_parts))
         ctx = mp.get_context("spawn")
         with ctx.Pool(cores, initializer=_batch_ref_init, initargs=(tmp,)) as pool:
-            pool.map(_batch_ref_one, list(range(min(cores, len(gs)))))  # warm-up: libraries loaded
+            # warm-up (libraries loaded); every wait is bounded
+            pool.map_async(_batch_ref_one, list(range(min(cores, len(gs))))).get(timeout=600)
             t0 = time.perf_counter()
-            res = pool.map(_batch_ref_one, list(range(len(gs))), chunksize=1)
+            res = pool.map_async(_batch_ref_one, list(range(len(gs))), chunksize=1).get(timeout=1200)
             wall = time.perf_counter() - t0
+    except mp.TimeoutError:
+        return {"value": None, "unit": "graphs/s", "cores": cores, "kind": "reference",
+                "sample": "unavailable: the reference's batched run did not finish within 20 minutes", "cuts": []}
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+    failed = sum(1 for r in res if r[1] is None)
     return {"value": len(gs) / wall, "unit": "graphs/s", "cores": cores, "kind": "reference",
             "sample": "all %d graphs, each partitioned by the reference's Serial build on one host core, %d at a "
-                      "time" % (len(gs), cores), "wall_s": wall, "cuts": [r[1] for r in res]}
+                      "time; %d of them the reference could not finish (it divides by zero in rebalance_weak when "
+                      "no part is undersized, src/jet_refiner.hpp:618)" % (len(gs), cores, failed),
+            "reference_failures": failed, "wall_s": wall, "cuts": [r[1] for r in res]}
 
 
 def _hbm_peak():
@@ -270,6 +289,15 @@ def run_only(args, wl, local):
     torch.cuda.set_device(local)
     jet = load_pkg()
     dev = torch.device("cuda", local)
+    if args.serving_only:
+        # the serving config on its own: one JSON line with the stream's
+        # capacity and its p50/p99 latency under Poisson arrivals
+        t0 = time.perf_counter()
+        sv = run_serving(jet, dev, args.serving, args.workers, 120 << 30, nmax=args.serving_nmax,
+                         pool=args.serving_pool, rates=[float(x) for x in args.serving_rates.split(",") if x])
+        print(json.dumps({"metric": "graphs/sec (serving)", "value": sv["all_at_once"]["graphs_per_s"], "unit": "graphs/s",
+                          "n_gpus": 1, "data": "synthetic", "wall_s": time.perf_counter() - t0, "serving": sv}), flush=True)
+        return
     g = wl["make"](jet.graphs, dev)
     k = wl["k"]
     level = 1
@@ -425,10 +453,12 @@ def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None, cpu_cores=0):
     lat = sorted(r[2] for r in res) or [0.0]
     edges = sum(g.nnz for g in gs) // 2
     cpu = None
+    stage("batched GPU legs done")
     if cpu_cores > 0 and ws == 1:
         cpu = run_batched_cpu(gs, cfgs, cpu_cores)
         cpu_cuts = cpu.pop("cuts")
-        cpu["cut_ratio_median"] = statistics.median(r[1] / max(c, 1) for r, c in zip(res, cpu_cuts))
+        ratios = [r[1] / max(c, 1) for r, c in zip(res, cpu_cuts) if c is not None]
+        cpu["cut_ratio_median"] = statistics.median(ratios) if ratios else None
     return {"cpu_baseline": cpu, "graphs": count, "graphs_this_rank": len(mine), "workers": workers,
             "sum_vertices_this_rank": sum(g.n for g in gs), "undirected_edges_this_rank": edges,
             "plain_graphs_per_s": count / t_plain, "batched_graphs_per_s": count / t_batch,
@@ -475,6 +505,26 @@ def finish_oracle_check(jet, chk):
             "oracle_seconds_one_thread": o["seconds"]}
 
 
+def check_full_size_fixture(g, part, cut):
+    """Compares a partition of R-MAT 2^24 with the oracle's, recorded in
+    tests/golden/rmat24_k256_oracle.json (the oracle takes about 12 minutes
+    on one host thread, too long to run here): same graph (SHA-256 of the
+    row offsets and neighbour ids), same cut, same part array (SHA-256)."""
+    import hashlib
+    path = os.path.join(ROOT, "tests", "golden", "rmat24_k256_oracle.json")
+    if not os.path.exists(path):
+        return None
+    want = json.load(open(path))
+    row, adj, _, _ = g.numpy()
+    same_graph = (hashlib.sha256(row.tobytes()).hexdigest() == want["row_sha256"] and
+                  hashlib.sha256(adj.tobytes()).hexdigest() == want["adj_sha256"])
+    p = part.cpu().numpy().astype("int32")
+    same_part = hashlib.sha256(p.tobytes()).hexdigest() == want["part_sha256"]
+    return {"fixture": "tests/golden/rmat24_k256_oracle.json", "same_graph": same_graph, "gpu_cut": cut,
+            "oracle_cut": want["cut"], "partition_equal": bool(same_graph and same_part and cut == want["cut"]),
+            "oracle_seconds_one_thread": want.get("oracle_seconds")}
+
+
 def run_powerlaw(jet, dev, scale, steps=2, cpu_scale=0, check=None):
     """The power-law config: R-MAT 2^scale (edge factor 8, symmetrised,
     de-duplicated, unit weights), int64 offsets and weights, 2-hop matching,
@@ -489,7 +539,7 @@ def run_powerlaw(jet, dev, scale, steps=2, cpu_scale=0, check=None):
     cfg = jet.config_t(coarsening_alg=0, num_parts=256, max_imb_ratio=1.10)
     jet.partition_big(cfg, g, seed=1)
     torch.cuda.synchronize()
-    times, last = [], None
+    times, last, first = [], None, None
     for s in range(steps):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -499,7 +549,10 @@ def run_powerlaw(jet, dev, scale, steps=2, cpu_scale=0, check=None):
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
         last = (cut, exp)
+        if s == 0:
+            first = (part, cut)
     cut, exp = last
+    full = check_full_size_fixture(g, first[0], first[1]) if scale == 24 else None
     # one more partition, untimed, with the library's events around every
     # level's table build (init_conn_data): the refinement kernel class that
     # events can bracket (the iteration kernels run inside graphs)
@@ -518,6 +571,7 @@ def run_powerlaw(jet, dev, scale, steps=2, cpu_scale=0, check=None):
                       "levels": v["launches"]}
     m = {k: v for k, v in zip(jet.MEASUREMENT_NAMES, exp.measurements)}
     sum_m = sum(cl.numEdges for cl in exp.coarseLevels) / 2
+    stage("power-law GPU legs done")
     cpu = None
     if cpu_scale > 0:
         _, ref = _oracle_mods()
@@ -529,9 +583,12 @@ def run_powerlaw(jet, dev, scale, steps=2, cpu_scale=0, check=None):
                "sample": "one partition of R-MAT 2^%d (same generator and settings, %d undirected edges) by the "
                          "reference's jet_host path, %.1f s" % (cpu_scale, ogs.row[-1] // 2, dt),
                "gpu_edges_per_s": (g.nnz / 2) / (statistics.median(times) / 1000.0)}
+    stage("power-law CPU sample done")
     chk = finish_oracle_check(jet, check) if check is not None else None
+    stage("oracle check done")
     refine_roof = run_class_profile(jet, jet.partition_big, cfg, g, 1, torch.cuda.current_stream())
-    return {"cpu_baseline": cpu, "oracle_check": chk, "refine_roofline": refine_roof, "workload": "rmat%d" % scale, "n": g.n, "undirected_edges": g.nnz // 2, "k": 256, "coarsening": "2-hop matching",
+    return {"cpu_baseline": cpu, "oracle_check": chk, "full_size_oracle_check": full, "refine_roofline": refine_roof,
+            "workload": "rmat%d" % scale, "n": g.n, "undirected_edges": g.nnz // 2, "k": 256, "coarsening": "2-hop matching",
             "imbalance": 1.10, "tier": "big", "ms_per_partition": statistics.median(times), "steps": steps,
             "edges_per_s": (g.nnz / 2) / (statistics.median(times) / 1000.0), "cut": cut, "imbalance_ratio": exp.imb_ratio,
             "levels": len(exp.coarseLevels),
@@ -543,41 +600,49 @@ def run_powerlaw(jet, dev, scale, steps=2, cpu_scale=0, check=None):
                                      "finest_level": tb.get("conn_build_finest"), "all_levels": tb.get("conn_build")}}
 
 
-def serving_workload(jet, dev, count, seed=5):
+def serving_workload(jet, dev, count, seed=5, nmax=1e6, pool=0):
     """Requests mixing 2D grids, random geometric graphs and R-MAT graphs:
-    n log-uniform in [1e4, 1e6], mean degree in [6, 16], k in {16..256}."""
+    n log-uniform in [1e4, nmax], mean degree in [6, 16], k in {16..256}.
+    With pool > 0 only `pool` distinct graphs are generated (each with its
+    own n, kind and degree drawn as above) and request i partitions graph
+    i mod pool with its own k and seed: the request mix keeps the config's
+    distributions while the device holds pool graphs, not count."""
     import random
     rng = random.Random(seed)
-    reqs = []
-    for i in range(count):
-        n = int(round(math.exp(rng.uniform(math.log(1e4), math.log(1e6)))))
+    distinct = count if pool <= 0 else min(pool, count)
+    gs = []
+    for i in range(distinct):
+        n = int(round(math.exp(rng.uniform(math.log(1e4), math.log(nmax)))))
         kind = rng.choice(["grid", "rgg", "rmat"])
-        k = rng.choice([16, 32, 64, 128, 256])
         deg = rng.uniform(6, 16)
         if kind == "grid":
             side = max(8, int(math.sqrt(n)))
             g = jet.graphs.grid2d(side, max(8, n // side), weighted=True, seed=i, device=dev)
-            cfg = jet.config_t(coarsening_alg=1, num_parts=k, max_imb_ratio=1.03)
         elif kind == "rgg":
             g = jet.graphs.rgg(n, deg, seed=i, device=dev)
-            cfg = jet.config_t(coarsening_alg=1, num_parts=k, max_imb_ratio=1.03)
         else:
             scale = max(10, int(round(math.log2(n))))
             g = jet.graphs.rmat(scale, max(2, int(deg / 2)), seed=i, tier="i32", device=dev)
-            cfg = jet.config_t(coarsening_alg=0, num_parts=k, max_imb_ratio=1.10)
-        reqs.append((cfg, g, i + 1))
+        gs.append((kind, g))
+    reqs = []
+    for i in range(count):
+        kind, g = gs[i % distinct]
+        k = rng.choice([16, 32, 64, 128, 256])
+        alg, imb = (0, 1.10) if kind == "rmat" else (1, 1.03)
+        reqs.append((jet.config_t(coarsening_alg=alg, num_parts=k, max_imb_ratio=imb), g, i + 1))
     return reqs
 
 
-def run_serving(jet, dev, count, workers, budget):
+def run_serving(jet, dev, count, workers, budget, nmax=1e6, pool=0, rates=(1.2, 0.5)):
     """A request stream through the server: first all at once (capacity),
-    then Poisson arrivals at 1.2x and 0.5x that capacity; latency is submit
-    to result."""
+    then Poisson arrivals at each of `rates` times that capacity; latency is
+    submit to result."""
     import random
     import torch
-    reqs = serving_workload(jet, dev, count)
+    reqs = serving_workload(jet, dev, count, nmax=nmax, pool=pool)
     torch.cuda.synchronize()
-    out = {"requests": count, "workers": workers, "budget_bytes": budget}
+    out = {"requests": count, "workers": workers, "budget_bytes": budget, "n_max": nmax,
+           "distinct_graphs": pool if 0 < pool < count else count}
 
     def stream(rate):
         srv = jet.Server("i32", workers=workers, mem_budget_bytes=budget)
@@ -603,8 +668,11 @@ def run_serving(jet, dev, count, workers, budget):
 
     cap, res0 = stream(None)
     out["all_at_once"] = cap
-    out["poisson_1.2x"], res1 = stream(1.2 * cap["graphs_per_s"])
-    out["poisson_0.5x"], _ = stream(0.5 * cap["graphs_per_s"])
+    res1 = res0
+    for j, r in enumerate(rates):
+        out["poisson_%gx" % r], rr = stream(r * cap["graphs_per_s"])
+        if j == 0:
+            res1 = rr
     cfg, g, sd = reqs[0]
     alone = jet.partition(cfg, g, seed=sd)
     out["same_alone_and_in_mix"] = bool(alone[1] == res0[0][1] == res1[0][1] and
@@ -629,6 +697,11 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--batched", type=int, default=512, help="graphs in the batched comparison (0 = skip)")
     ap.add_argument("--serving", type=int, default=96, help="requests in the serving run (0 = skip)")
+    ap.add_argument("--serving-nmax", type=float, default=1e6, help="largest request graph (vertices)")
+    ap.add_argument("--serving-pool", type=int, default=0,
+                    help="distinct graphs the requests cycle through (0 = one graph per request)")
+    ap.add_argument("--serving-rates", default="1.2,0.5", help="Poisson loads as multiples of the measured capacity")
+    ap.add_argument("--serving-only", action="store_true", help="run the serving stream alone (no other legs)")
     ap.add_argument("--workers", type=int, default=16)
     ap.add_argument("--powerlaw-scale", type=int, default=24, help="R-MAT scale of the power-law run (0 = skip)")
     ap.add_argument("--check-scale", type=int, default=20,
@@ -661,6 +734,15 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     jet = load_pkg()
     dev = torch.device("cuda", local)
+    if args.serving_only:
+        # the serving config on its own: one JSON line with the stream's
+        # capacity and its p50/p99 latency under Poisson arrivals
+        t0 = time.perf_counter()
+        sv = run_serving(jet, dev, args.serving, args.workers, 120 << 30, nmax=args.serving_nmax,
+                         pool=args.serving_pool, rates=[float(x) for x in args.serving_rates.split(",") if x])
+        print(json.dumps({"metric": "graphs/sec (serving)", "value": sv["all_at_once"]["graphs_per_s"], "unit": "graphs/s",
+                          "n_gpus": 1, "data": "synthetic", "wall_s": time.perf_counter() - t0, "serving": sv}), flush=True)
+        return
     g = wl["make"](jet.graphs, dev)
     cfg = jet.config_t(coarsening_alg=wl["alg"], num_parts=wl["k"], max_imb_ratio=wl["imb"])
     part_fn = getattr(jet, PART_FN[wl["tier"]])
@@ -704,7 +786,9 @@ def main():
         dist.barrier()
     value = ws * args.steps / (max_total_ms / 1000.0)
 
+    stage("timed region done: %.2f ms per step" % (sum(times) / len(times)))
     class_prof = run_class_profile(jet, part_fn, cfg, g, 1, stream) if rank == 0 else None
+    stage("class profile done")
 
     # end to end through the C ABI with host buffers (copies in the timed region)
     host_fn = getattr(jet, HOST_FN[wl["tier"]])
@@ -723,6 +807,7 @@ def main():
     h2d = (g.n + 1) * eb + g.nnz * (ob + wb) + g.n * wb
     d2h = g.n * 4
     e2e_value = ws * len(e2e_times) / sum(e2e_times) if e2e_times else None
+    stage("e2e done")
     cpu_cores = 0
     if ws == 1 and not args.no_cpu_baseline:
         cpu_cores = _oracle_mods()[1].concurrency("host")
@@ -730,7 +815,12 @@ def main():
     if args.powerlaw_scale > 0 and args.check_scale > 0 and rank == 0:
         chk = start_oracle_check(jet, dev, args.check_scale)
     batched = run_batched(jet, dev, args.batched, args.workers, ws, rank, dist, cpu_cores) if args.batched > 0 else None
-    serving = run_serving(jet, dev, args.serving, args.workers, 120 << 30) if args.serving > 0 and rank == 0 else None
+    stage("batched done")
+    serving = None
+    if args.serving > 0 and rank == 0:
+        serving = run_serving(jet, dev, args.serving, args.workers, 120 << 30, nmax=args.serving_nmax,
+                              pool=args.serving_pool, rates=[float(x) for x in args.serving_rates.split(",") if x])
+    stage("serving done")
     powerlaw = None
     if args.powerlaw_scale > 0 and rank == 0:
         powerlaw = run_powerlaw(jet, dev, args.powerlaw_scale, cpu_scale=(args.powerlaw_scale - 3) if cpu_cores else 0,
@@ -770,9 +860,11 @@ def main():
             roof = dict(tb, bound="hbm", peak=hbm_peak, peak_source=peak_src, unit="GB/s")
         else:
             roof["finest_table_build"] = tb
+    stage("power-law done")
     cpu_base = None
     if ws == 1 and not args.no_cpu_baseline:
         dt, ocut, oimb = reference_partition(host_graph(g), wl, 1)
+        stage("CPU baseline done")
         cpu_base = {"value": 1.0 / dt, "unit": "graphs/s", "cores": cpu_cores, "kind": "reference",
                     "sample": "one full partition of the same graph by the reference's jet_host path on %d OpenMP "
                               "threads, cut %d" % (cpu_cores, ocut)}

@@ -293,6 +293,9 @@ int jet_test_table_overflow(int cap, int k, int nparts, int* claimed);
  * jet_copy copies between any two host or device pointers (cudaMemcpyDefault). */
 int jet_device_alloc(int64_t bytes, void** ptr);
 
+int jet_device_free(void* ptr);
+int jet_copy(void* dst, const void* src, int64_t bytes);
+
 /* METIS text graph reader with the reference's rules (app/io.hpp:99-217),
  * parsed in parallel on `threads` host threads (0 = all cores).  Allocates
  * row_map[n+1], entries[nnz] and values[nnz] in host memory in the tier's
@@ -302,8 +305,6 @@ int jet_device_alloc(int64_t bytes, void** ptr);
 int jet_read_metis(const char* path, int tier, int threads, int64_t* n, int64_t* nnz, void** row_map, void** entries,
                    void** values, int* uniform_ew);
 void jet_free_host(void* ptr);
-int jet_device_free(void* ptr);
-int jet_copy(void* dst, const void* src, int64_t bytes);
 
 /* Level-loop drivers refinement may use, process-wide (no counterpart in the
  * reference, whose loop is always host-driven, src/jet_refiner.hpp:1094-1134).
@@ -312,13 +313,17 @@ int jet_copy(void* dst, const void* src, int64_t bytes);
  * clusters are not allowed; nnz <= 262144; k <= 256), one thread-block
  * cluster of 8-16 CTAs (n <= 65536, nnz <= 2^21, k <= 512), one cooperative
  * grid kernel (n <= 131072, nnz <= 2^21, k <= 512), a CUDA graph with
- * conditional nodes, else the host loop.  Returns the previous mask. */
+ * conditional nodes, else the host loop.  JET_DRIVER_CTA_SMEM lets the
+ * one-CTA loop keep the level's mutable state in shared memory (as much of
+ * it as fits); without it that state stays in global memory.  Returns the
+ * previous mask. */
 enum {
     JET_DRIVER_CTA = 1,
     JET_DRIVER_COOP = 2,
     JET_DRIVER_GRAPH = 4,
     JET_DRIVER_CLUSTER = 8,
-    JET_DRIVER_ALL = 15
+    JET_DRIVER_CTA_SMEM = 16,
+    JET_DRIVER_ALL = 31
 };
 int jet_set_refine_drivers(int mask);
 

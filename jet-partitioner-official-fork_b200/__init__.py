@@ -62,7 +62,7 @@ EXPORTED_SYMBOLS = [
 ]
 
 # level-loop drivers (jet_set_refine_drivers)
-DRIVER_CTA, DRIVER_COOP, DRIVER_GRAPH, DRIVER_CLUSTER, DRIVER_ALL = 1, 2, 4, 8, 15
+DRIVER_CTA, DRIVER_COOP, DRIVER_GRAPH, DRIVER_CLUSTER, DRIVER_CTA_SMEM, DRIVER_ALL = 1, 2, 4, 8, 16, 31
 
 
 class JetError(RuntimeError):

@@ -144,6 +144,8 @@ void count_launch();
 int64_t launch_counter();
 // Which level-loop drivers refinement may use (JET_DRIVER_* bits).
 int refine_drivers();
+// The one-CTA level loop may keep its state in shared memory (JET_DRIVER_CTA_SMEM).
+bool cta_smem_resident();
 // JET_DEBUG_TIMING set in the environment: phase timings go to stderr.
 bool debug_timing();
 // Host clock in milliseconds (steady).

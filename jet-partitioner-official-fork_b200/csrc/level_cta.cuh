@@ -107,14 +107,63 @@ __device__ __forceinline__ void cta_zero_buckets(const RebArgs<O, W>& rb) {
     __syncthreads();
 }
 
+// Where the single-CTA loop keeps the level's mutable state.  The loop is
+// bound by the latency of its dependent accesses, phase after phase; arrays
+// placed in shared memory (byte offsets past the phase scratch at offset 0)
+// are read and written there for the whole loop instead of through L2.
+// NO_SMEM leaves an array in global memory.  Only the single CTA of the
+// launch touches these arrays, so moving them cannot change a result.
+static constexpr uint32_t NO_SMEM = 0xffffffffu;
+struct CtaSmemPlan {
+    uint32_t part, dest, csize, dest_cache, save_gain, pregain, lock, mark;
+    uint32_t cand, moves, bid, score, sizes, dev, ctl, slots, buckets, boff;
+    int64_t nslots, nbuckets;
+    size_t total;  // dynamic shared memory the launch needs
+};
+
+template <class T>
+__device__ __forceinline__ void cta_place(unsigned char* base, uint32_t off, T*& ptr, int64_t count) {
+    if (off == NO_SMEM) return;
+    T* dst = (T*)(base + off);
+    const T* src = ptr;
+    for (int64_t i = threadIdx.x; i < count; i += blockDim.x) dst[i] = src[i];
+    ptr = dst;
+}
+
 template <class O, class E, class W>
 __global__ void __launch_bounds__(CTA_THREADS, 1)
 k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, W> rbs, Ctl<W>* c, part_t* best_part,
-            W* sizes_best, int P, int max_iters) {
+            W* sizes_best, int P, int max_iters, CtaSmemPlan plan) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint64_t* keys = (uint64_t*)smem_raw;
     __shared__ int s_mode, s_more, s_copy;
     const O n = a.g.n;
+    Ctl<W>* const c_global = c;
+    RefDev<O, W>* const dev_global = a.dev;
+    {
+        // move the planned arrays into shared memory
+        cta_place(smem_raw, plan.part, a.part, n);
+        cta_place(smem_raw, plan.dest, a.dest, n);
+        cta_place(smem_raw, plan.csize, a.csize, n);
+        cta_place(smem_raw, plan.dest_cache, a.dest_cache, n);
+        cta_place(smem_raw, plan.save_gain, a.save_gain, n);
+        cta_place(smem_raw, plan.pregain, a.pregain, n);
+        cta_place(smem_raw, plan.lock, a.lock, n);
+        cta_place(smem_raw, plan.mark, a.mark, n);
+        cta_place(smem_raw, plan.cand, a.cand, n);
+        cta_place(smem_raw, plan.moves, a.moves, n);
+        cta_place(smem_raw, plan.sizes, a.sizes, a.k);
+        cta_place(smem_raw, plan.dev, a.dev, 1);
+        cta_place(smem_raw, plan.ctl, c, 1);
+        cta_place(smem_raw, plan.slots, a.slots, plan.nslots);
+        cta_place(smem_raw, plan.bid, rbw.bid, n);
+        cta_place(smem_raw, plan.score, rbw.score, n);
+        cta_place(smem_raw, plan.buckets, rbw.buckets, plan.nbuckets);
+        cta_place(smem_raw, plan.boff, rbw.boff, plan.nbuckets);
+        rbs.bid = rbw.bid; rbs.score = rbw.score; rbs.buckets = rbw.buckets; rbs.boff = rbw.boff;
+        if (plan.ctl != NO_SMEM) a.filter = &c->filter;
+        __syncthreads();
+    }
     if (threadIdx.x == 0) {
         ctl_begin_logic(c);
         s_mode = c->mode;
@@ -196,7 +245,56 @@ k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, 
         }
         __syncthreads();
     }
+    // the host reads the control state and the error flags after the level
+    if (threadIdx.x == 0) {
+        if (plan.ctl != NO_SMEM) *c_global = *c;
+        if (plan.dev != NO_SMEM && a.dev->err) atomicOr(&dev_global->err, a.dev->err);
+    }
 }
+
+// Places the loop's arrays in shared memory, most latency-critical first,
+// while they fit beside the phase scratch; the rest stay in global memory.
+template <class O, class W>
+inline CtaSmemPlan plan_cta_smem(int64_t n, int64_t nslots, int64_t nbuckets, int k, size_t scratch, size_t budget,
+                                 bool enable) {
+    CtaSmemPlan pl;
+    uint32_t* fields[] = {&pl.part, &pl.dest, &pl.csize, &pl.dest_cache, &pl.save_gain, &pl.pregain, &pl.lock, &pl.mark,
+                          &pl.cand, &pl.moves, &pl.bid, &pl.score, &pl.sizes, &pl.dev, &pl.ctl, &pl.slots,
+                          &pl.buckets, &pl.boff};
+    for (uint32_t* f : fields) *f = NO_SMEM;
+    pl.nslots = nslots;
+    pl.nbuckets = nbuckets;
+    pl.total = scratch;
+    if (!enable) return pl;
+    size_t off = (scratch + 15) & ~(size_t)15;
+    auto take = [&](uint32_t& f, size_t bytes) {
+        size_t end = off + ((bytes + 15) & ~(size_t)15);
+        if (end > budget) return;
+        f = (uint32_t)off;
+        off = end;
+    };
+    take(pl.dev, sizeof(RefDev<O, W>));
+    take(pl.ctl, sizeof(Ctl<W>));
+    take(pl.sizes, (size_t)k * sizeof(W));
+    take(pl.part, n * sizeof(part_t));
+    take(pl.dest, n * sizeof(part_t));
+    take(pl.csize, n * sizeof(part_t));
+    take(pl.dest_cache, n * sizeof(part_t));
+    take(pl.lock, n);
+    take(pl.mark, n);
+    take(pl.pregain, n * sizeof(W));
+    take(pl.save_gain, n * sizeof(W));
+    take(pl.slots, nslots * sizeof(Slot<W>));
+    take(pl.cand, n * sizeof(O));
+    take(pl.moves, n * sizeof(O));
+    take(pl.bid, n * sizeof(O));
+    take(pl.score, n * sizeof(W));
+    take(pl.buckets, nbuckets * sizeof(W));
+    take(pl.boff, nbuckets * sizeof(W));
+    pl.total = off;
+    return pl;
+}
+
 
 template <class O, class W>
 constexpr size_t level_cta_smem(int P, int k) {

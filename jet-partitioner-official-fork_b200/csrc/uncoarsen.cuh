@@ -716,12 +716,19 @@ struct Refiner {
         RebArgs<O, W> rbs = reb_args(L, strong_max_dest(pb.opt, pb.size_max), pb.opt, pb.size_max, false);
         int P = 1;
         while (P < (int)L.n) P <<= 1;
-        size_t smem = level_cta_smem<O, W>(P, k) + 64;
+        size_t scratch = level_cta_smem<O, W>(P, k) + 64;
         // the attribute is per function and process-wide: always the device
         // maximum, so concurrent callers with different sizes cannot race
-        JET_CUDA(cudaFuncSetAttribute(k_level_cta<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      max_dynamic_smem((const void*)k_level_cta<O, E, W>)));
-        k_level_cta<O, E, W><<<1, CTA_THREADS, smem, s>>>(args(L), li, rbw, rbs, ctl.p, best_part, sizes_best.p, P, 1 << 22);
+        const size_t smax = max_dynamic_smem((const void*)k_level_cta<O, E, W>);
+        JET_CUDA(cudaFuncSetAttribute(k_level_cta<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+        // the level's table slots: the capacities' total (coff[n]) as init_conn left it
+        JET_CUDA(cudaMemcpyAsync(e.hscal, coff.p + L.n, sizeof(E), cudaMemcpyDeviceToHost, s));
+        e.sync();
+        const int64_t nslots = (int64_t)*(E*)e.hscal;
+        const int64_t nbuckets = (int64_t)rbw.t_minibuckets + 1 + rbw.width;
+        CtaSmemPlan plan = plan_cta_smem<O, W>((int64_t)L.n, nslots, nbuckets, k, scratch, smax, cta_smem_resident());
+        k_level_cta<O, E, W><<<1, CTA_THREADS, plan.total, s>>>(args(L), li, rbw, rbs, ctl.p, best_part, sizes_best.p, P,
+                                                                 1 << 22, plan);
         count_launch();
         JET_LAUNCH_CHECK();
         ctl_finish();

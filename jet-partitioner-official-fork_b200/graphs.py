@@ -137,23 +137,56 @@ def grid3d(nx: int, ny: int, nz: int, weighted: bool = True, seed: int = 1, tier
     return from_undirected(nx * ny * nz, u, v, w, tier)
 
 
+_M63 = 1 << 63
+
+
+def _s64(c: int) -> int:
+    """A 64-bit constant as the int64 with the same bits."""
+    return c - (1 << 64) if c >= _M63 else c
+
+
+_SM0, _SM1, _SM2 = _s64(0x9E3779B97F4A7C15), _s64(0xBF58476D1CE4E5B9), _s64(0x94D049BB133111EB)
+
+
+def _srl(x: torch.Tensor, s: int) -> torch.Tensor:
+    """Logical right shift of int64 bit patterns."""
+    return (x >> s) & ((1 << (64 - s)) - 1)
+
+
+def _mix64(x: torch.Tensor) -> torch.Tensor:
+    """splitmix64 (S. Vigna) on int64 bit patterns: wrapping integer
+    arithmetic, identical on every device."""
+    x = x + _SM0
+    x = (x ^ _srl(x, 30)) * _SM1
+    x = (x ^ _srl(x, 27)) * _SM2
+    return x ^ _srl(x, 31)
+
+
+def _uniform(seed: int, idx: torch.Tensor) -> torch.Tensor:
+    """Doubles in [0, 1) from the counter idx under seed (53 random bits)."""
+    key = _mix64(torch.full_like(idx, _s64(seed & ((1 << 64) - 1)))) ^ idx
+    return _srl(_mix64(key), 11).to(torch.float64) * (1.0 / (1 << 53))
+
+
 def rmat(scale: int, edge_factor: int = 8, a: float = 0.57, b: float = 0.19, c: float = 0.19,
          seed: int = 1, tier: str = "big", device="cpu", chunk: int = 1 << 25) -> CSRGraph:
     """R-MAT with 2^scale vertices and edge_factor * 2^scale sampled edges,
-    symmetrised, de-duplicated, self-loops removed, unit weights."""
+    symmetrised, de-duplicated, self-loops removed, unit weights.  Every
+    random number is a counter-based hash of (seed, edge, bit), so the graph
+    is the same on every device."""
     n = 1 << scale
     m = edge_factor * n
-    gen = _gen(seed, device)
     probs = torch.tensor([a, b, c, 1.0 - a - b - c], device=device, dtype=torch.float64)
     cum = torch.cumsum(probs, 0)
     keys = []
     done = 0
     while done < m:
         cnt = min(chunk, m - done)
+        eidx = (torch.arange(cnt, dtype=torch.int64, device=device) + done) * 64
         u = torch.zeros(cnt, dtype=torch.int64, device=device)
         v = torch.zeros(cnt, dtype=torch.int64, device=device)
         for bit in range(scale):
-            r = torch.rand(cnt, generator=gen, device=device, dtype=torch.float64)
+            r = _uniform(seed, eidx + bit)
             q = torch.searchsorted(cum, r, right=True).clamp_(max=3)
             u |= (q >> 1) << bit
             v |= (q & 1) << bit

@@ -28,6 +28,19 @@ _REF_SRC = "/root/reference"
 _loaded = {}
 
 
+class ReferenceCrash(RuntimeError):
+    """The reference raised SIGFPE: its rebalance_weak divides by zero when no
+    part is undersized (src/jet_refiner.hpp:618)."""
+
+
+def _rc(rc: int, what: str):
+    if rc == 8:
+        raise ReferenceCrash("the reference's %s raised SIGFPE (division by zero in rebalance_weak, "
+                             "src/jet_refiner.hpp:618)" % what)
+    if rc != 0:
+        raise RuntimeError("reference %s failed with code %d" % (what, rc))
+
+
 def available(space: str = "serial") -> bool:
     """True when the library is built, or can be built because the reference
     sources are present on this machine."""
@@ -68,8 +81,7 @@ def partition(g: G, k: int, alg: int = 1, imb: float = 1.03, seed: int = 1, tol:
                                   ctypes.c_int64(g.n), _p(g.row), _p(g.adj), _p(g.val), _p(g.vw), int(g.uniform),
                                   ctypes.c_uint64(seed), _p(part), ctypes.byref(cut), ctypes.byref(imb_out),
                                   ctypes.byref(secs), 1)
-    if rc != 0:
-        raise RuntimeError("reference partition failed with code %d" % rc)
+    _rc(rc, "partition")
     return part, int(cut.value), float(imb_out.value), float(secs.value)
 
 
@@ -130,7 +142,7 @@ def refine_iters(g: G, part, k: int, imb: float, filter_ratio: float, iters: int
                                      _p(part), k, ctypes.c_double(imb), ctypes.c_double(filter_ratio), iters,
                                      _p(sizes), ctypes.byref(cut), _p(off), _p(ent), _p(cval), _p(size), _p(dc),
                                      _p(moves), _p(kinds))
-    assert rc == 0
+    _rc(rc, "refinement iterations")
     c = int(off[-1])
     return dict(part=part, sizes=sizes, cut=int(cut.value), off=off, ent=ent[:c].copy(), val=cval[:c].copy(),
                 size=size, dest_cache=dc, moves=moves[:iters], kinds=kinds[:iters])
@@ -144,7 +156,7 @@ def refine_level(g: G, part, k: int, imb: float = 1.03, tol: float = 0.999, ultr
     rc = lib(space).ref_refine_level(g.tier, ctypes.c_int64(g.n), _p(g.row), _p(g.adj), _p(g.val), _p(g.vw),
                                      _p(part), k, ctypes.c_double(imb), ctypes.c_double(tol), int(ultra),
                                      int(g.uniform), ctypes.byref(cut), ctypes.byref(it))
-    assert rc == 0
+    _rc(rc, "jet_refine")
     return part, int(cut.value)
 
 
@@ -165,7 +177,7 @@ def uncoarsen(levels, maps, coarsest_part, k: int, imb: float = 1.03, tol: float
                                   arr([lv.val for lv in levels]), arr([lv.vw for lv in levels]), arr(mp), _p(cp), k,
                                   ctypes.c_double(imb), ctypes.c_double(tol), int(ultra), int(levels[0].uniform),
                                   _p(part), ctypes.byref(cut))
-    assert rc == 0
+    _rc(rc, "uncoarsen")
     return part, int(cut.value)
 
 

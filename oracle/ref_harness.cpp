@@ -19,6 +19,9 @@
 #include <fcntl.h>
 #include <unistd.h>
 
+#include <csetjmp>
+#include <csignal>
+
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
@@ -62,6 +65,42 @@ struct Quiet {
         close(saved);
     }
 };
+
+// The reference divides by zero in rebalance_weak when no part is undersized
+// (src/jet_refiner.hpp:618), which raises SIGFPE.  A call made under
+// FPE_GUARD turns that into status REF_SIGFPE when the fault is on the
+// calling thread (always so for the Serial build); the reference's
+// allocations of the abandoned call are leaked.
+static constexpr int REF_SIGFPE = 8;
+thread_local sigjmp_buf* t_fpe_jmp = nullptr;
+void on_fpe(int sig) {
+    if (t_fpe_jmp) siglongjmp(*t_fpe_jmp, sig);
+    std::signal(sig, SIG_DFL);
+    std::raise(sig);
+}
+struct FpeHandler {
+    struct sigaction old {};
+    FpeHandler() {
+        struct sigaction sa {};
+        sa.sa_handler = on_fpe;
+        sigemptyset(&sa.sa_mask);
+        sa.sa_flags = SA_NODEFER;
+        sigaction(SIGFPE, &sa, &old);
+    }
+    ~FpeHandler() { sigaction(SIGFPE, &old, nullptr); }
+};
+#define FPE_GUARD(...)                                 \
+    {                                                  \
+        FpeHandler fpe_handler_;                       \
+        sigjmp_buf fpe_jb_;                            \
+        if (sigsetjmp(fpe_jb_, 1)) {                   \
+            t_fpe_jmp = nullptr;                       \
+            return REF_SIGFPE;                         \
+        }                                              \
+        t_fpe_jmp = &fpe_jb_;                          \
+        __VA_ARGS__;                                   \
+        t_fpe_jmp = nullptr;                           \
+    }
 
 template <class T, class V>
 V to_view(const void* src, int64_t n, const char* label) {
@@ -123,7 +162,9 @@ int ref_concurrency() { return RefSpace().concurrency(); }
 // partitioner::partition (src/partitioner.hpp:61-125) through the reference's
 // own entry instantiation.  The coarsening RNG pool is seeded with `seed`
 // (the reference seeds it from the clock, src/contract.hpp:503).
-// Returns 0; *seconds_out is the wall time of the partition call alone.
+// Returns 0, or 8 when the reference raised SIGFPE (its division by zero in
+// rebalance_weak, src/jet_refiner.hpp:618); *seconds_out is the wall time of
+// the partition call alone.
 int ref_partition(int tier, int alg, int k, double imb, double tol, int ultra, int64_t n, const void* row,
                   const void* adj, const void* val, const void* vw, int uniform_ew, uint64_t seed, int32_t* part_out,
                   int64_t* cut_out, double* imb_out, double* seconds_out, int quiet) {
@@ -135,8 +176,9 @@ int ref_partition(int tier, int alg, int k, double imb, double tol, int ultra, i
         experiment_data<W> exp;
         W cut = 0;
         Quiet q(quiet != 0);
+        typename partitioner<Mat<O, E, W>, part_t>::part_vt part;
         auto t0 = std::chrono::steady_clock::now();
-        auto part = partitioner<Mat<O, E, W>, part_t>::partition(cut, cfg, g, w, uniform_ew != 0, exp);
+        FPE_GUARD(part = partitioner<Mat<O, E, W>, part_t>::partition(cut, cfg, g, w, uniform_ew != 0, exp));
         auto t1 = std::chrono::steady_clock::now();
         std::memcpy(part_out, part.data(), (size_t)n * sizeof(int32_t));
         *cut_out = (int64_t)cut;
@@ -266,7 +308,7 @@ int ref_refine_iters(int tier, int64_t n, const void* row, const void* adj, cons
                 bal = 0;
                 kind = 0;
             } else if (bal < 2) {
-                moves = r.rebalance_weak(prob, p, cd, r.perm_scratch, st.part_sizes);
+                FPE_GUARD(moves = r.rebalance_weak(prob, p, cd, r.perm_scratch, st.part_sizes));
                 bal++;
                 kind = 1;
             } else {
@@ -309,7 +351,7 @@ int ref_refine_level(int tier, int64_t n, const void* row, const void* adj, cons
         experiment_data<W> exp;
         {
             Quiet q(true);
-            r.jet_refine(g, cfg, w, p, uniform_ew != 0, st, exp);
+            FPE_GUARD(r.jet_refine(g, cfg, w, p, uniform_ew != 0, st, exp));
         }
         std::memcpy(part, p.data(), (size_t)n * sizeof(int32_t));
         *cut_out = (int64_t)st.cut;
@@ -349,7 +391,8 @@ int ref_uncoarsen(int tier, int nlevels, const int64_t* ns, const void* const* r
         experiment_data<W> exp;
         W cut = 0;
         Quiet q(true);
-        auto part = U::uncoarsen(levels, cp, cfg, cut, exp);
+        typename U::part_vt part;
+        FPE_GUARD(part = U::uncoarsen(levels, cp, cfg, cut, exp));
         std::memcpy(part_out, part.data(), (size_t)ns[0] * sizeof(int32_t));
         *cut_out = (int64_t)cut;
         return 0;

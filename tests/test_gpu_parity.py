@@ -318,15 +318,15 @@ def test_edge_cases(jet, graphs, orc):
     assert orc.pstat(orc.G.from_csr(small), p, 3)[0] == cut
 
 
-@pytest.mark.parametrize("drivers", ["all", "cluster", "coop", "graph", "host"])
+@pytest.mark.parametrize("drivers", ["all", "cta_global", "cluster", "coop", "graph", "host"])
 @pytest.mark.parametrize("tier,kind,k", [("i32", "grid2d", 16), ("big", "rgg", 64), ("biggest", "grid2d", 300),
                                          ("i32", "rgg", 600)])
 def test_level_drivers_bit_exact(jet, graphs, orc, drivers, tier, kind, k):
-    """Every level-loop driver (one CTA, one thread-block cluster, cooperative
-    grid kernel, CUDA graph with conditional nodes, host loop) returns the
-    oracle's partition on graphs whose finer levels exceed the one-CTA
-    bound."""
-    mask = {"all": jet.DRIVER_ALL, "cluster": jet.DRIVER_CLUSTER, "coop": jet.DRIVER_COOP | jet.DRIVER_GRAPH,
+    """Every level-loop driver (one CTA with its state in shared or in global
+    memory, one thread-block cluster, cooperative grid kernel, CUDA graph
+    with conditional nodes, host loop) returns the oracle's partition on
+    graphs whose finer levels exceed the one-CTA bound."""
+    mask = {"all": jet.DRIVER_ALL, "cta_global": jet.DRIVER_CTA, "cluster": jet.DRIVER_CLUSTER, "coop": jet.DRIVER_COOP | jet.DRIVER_GRAPH,
             "graph": jet.DRIVER_GRAPH, "host": 0}[drivers]
     g = graphs.grid2d(170, 150, weighted=True, seed=7) if kind == "grid2d" else graphs.rgg(30000, 9.0, seed=5)
     g = g.as_tier(tier)
@@ -531,3 +531,51 @@ def test_gpu_matches_reference_directly(jet, graphs, orc, ref, tier, kind, k):
     assert np.array_equal(host(got["part"]), want["part"])
     assert np.array_equal(host(got["sizes"]), want["sizes"])
     assert got["cut"] == want["cut"]
+
+
+def test_class_profiling_pass_leaves_results_unchanged(jet, graphs, orc):
+    """The profiling pass (every level on the host-driven loop, event brackets
+    per kernel class, device-side counts for the byte model) returns the same
+    partition as a normal call, and accounts time and bytes to the classes
+    that ran."""
+    g = graphs.grid3d(40, 40, 30, weighted=True, seed=4)
+    og = orc.G.from_csr(g)
+    cfg = jet.config_t(coarsening_alg=1, num_parts=16, max_imb_ratio=1.03)
+    want, wcut, _ = orc.partition(og, 16, alg=1, imb=1.03, seed=2)
+    prev = jet.set_refine_drivers(0)
+    try:
+        jet.prof_enable(True)
+        part, cut, _ = jet.partition(cfg, g.to("cuda"), seed=2)
+        torch.cuda.synchronize()
+        prof = jet.prof_read()
+        jet.prof_enable(False)
+    finally:
+        jet.set_refine_drivers(prev)
+    assert cut == wcut and np.array_equal(host(part), want)
+    for c in ("conn_build", "lp_select", "afterburn", "apply", "cut_after"):
+        assert prof[c]["launches"] > 0 and prof[c]["ms"] > 0 and prof[c]["bytes"] > 0, (c, prof[c])
+    assert prof["update"]["launches"] > 0
+
+
+def test_rmat24_k256_full_size_equals_oracle_fixture(jet, graphs):
+    """The power-law config at full size -- R-MAT 2^24, k = 256, 2-hop,
+    imbalance 1.10, int64 offsets and weights -- against the oracle's
+    partition recorded in tests/golden/rmat24_k256_oracle.json (made by
+    tests/golden/make_rmat24_fixture.py; the oracle needs about 12 minutes on
+    one host thread).  The graph is generated on the GPU by the same
+    counter-based generator and checked against the fixture's digests."""
+    import hashlib
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rmat24_k256_oracle.json")
+    if not os.path.exists(path):
+        pytest.skip("fixture not generated")
+    want = json.load(open(path))
+    g = graphs.rmat(24, 8, seed=1, tier="big", device="cuda")
+    assert hashlib.sha256(host(g.row).tobytes()).hexdigest() == want["row_sha256"]
+    assert hashlib.sha256(host(g.adj).tobytes()).hexdigest() == want["adj_sha256"]
+    cfg = jet.config_t(coarsening_alg=0, num_parts=256, max_imb_ratio=1.10)
+    part, cut, exp = jet.partition_big(cfg, g, seed=1)
+    assert cut == want["cut"]
+    assert hashlib.sha256(host(part).astype(np.int32).tobytes()).hexdigest() == want["part_sha256"]
+    assert exp.imb_ratio <= 1.10 + 1e-12

@@ -235,3 +235,19 @@ def test_quality_within_two_percent_of_reference(graphs):
         theirs.append(rc)
         assert ref.pstat(g, rp, k)[0] == rc
     assert np.median(mine) <= 1.02 * np.median(theirs), (mine, theirs)
+
+
+def test_reference_divides_by_zero_where_the_oracle_does_not(graphs):
+    """A documented deviation: with no undersized part, the reference's
+    rebalance_weak computes i % 0 (src/jet_refiner.hpp:618) and the process
+    dies of SIGFPE; here the vertex stays in place.  Graph 334 of the batched
+    config (a 1,145-vertex random geometric graph, k = 64) reaches that
+    state."""
+    g = orc.G.from_csr(graphs.rgg(1145, 10.0, seed=334))
+    with pytest.raises(ref.ReferenceCrash):
+        ref.partition(g, 64, alg=1, imb=1.03, seed=335)
+    part, cut, st = orc.partition(g, 64, alg=1, imb=1.03, seed=335)
+    assert part.min() >= 0 and part.max() < 64
+    assert orc.pstat(g, part, 64)[0] == cut
+    # the reference's library keeps working after the caught fault
+    assert ref.partition(g, 8, alg=1, imb=1.03, seed=1)[1] > 0
