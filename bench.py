@@ -470,39 +470,58 @@ def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None, cpu_cores=0):
 POWERLAW = dict(k=256, alg=0, imb=1.10, tier="big")
 
 
+def _oracle_check_worker(path, out_path):
+    """Child process of start_oracle_check: the oracle's partition of the
+    graph stored at `path`, written to `out_path`."""
+    import numpy as np
+    oracle, _ = _oracle_mods()
+    arr = [np.load(path + "_%s.npy" % nm) for nm in ("row", "adj", "val", "vw")]
+    og = oracle.G(*arr, uniform=True)
+    t = time.perf_counter()
+    part, cut, _ = oracle.partition(og, POWERLAW["k"], alg=POWERLAW["alg"], imb=POWERLAW["imb"], seed=1)
+    np.save(out_path + "_part.npy", part)
+    with open(out_path + "_meta.json", "w") as f:
+        json.dump({"cut": int(cut), "seconds": time.perf_counter() - t}, f)
+
+
 def start_oracle_check(jet, dev, scale):
     """Starts the oracle's partition of R-MAT 2^scale (the power-law config at
-    a size one host thread finishes in well under a minute) on a background
-    thread; the GPU's partition of the same graph is compared with it at the
-    end of the power-law run.  The oracle call releases the interpreter lock,
-    so it overlaps the GPU work that follows."""
-    import threading
+    a size one host thread finishes in well under a minute) in a child
+    process; the GPU's partition of the same graph is compared with it at the
+    end of the power-law run.  A separate process, not a thread: Metis keeps
+    global state, and an oracle call in this process would share it with the
+    library's own Metis calls made meanwhile."""
+    import multiprocessing as mp
+    import numpy as np
     g = jet.graphs.rmat(scale, 8, seed=1, tier="big", device=dev)
-    og = host_graph(g)
-    oracle, _ = _oracle_mods()
-    out = {}
-
-    def work():
-        t = time.perf_counter()
-        out["part"], out["cut"], _ = oracle.partition(og, POWERLAW["k"], alg=POWERLAW["alg"], imb=POWERLAW["imb"],
-                                                      seed=1)
-        out["seconds"] = time.perf_counter() - t
-
-    th = threading.Thread(target=work, daemon=True)
-    th.start()
-    return {"graph": g, "scale": scale, "thread": th, "out": out}
+    tmp = tempfile.mkdtemp(prefix="jet_check_")
+    base = os.path.join(tmp, "g")
+    for nm, a in zip(("row", "adj", "val", "vw"), g.numpy()):
+        np.save(base + "_%s.npy" % nm, a)
+    proc = mp.get_context("spawn").Process(target=_oracle_check_worker, args=(base, base))
+    proc.start()
+    return {"graph": g, "scale": scale, "proc": proc, "dir": tmp, "base": base}
 
 
 def finish_oracle_check(jet, chk):
+    import shutil
     import numpy as np
     cfg = jet.config_t(coarsening_alg=POWERLAW["alg"], num_parts=POWERLAW["k"], max_imb_ratio=POWERLAW["imb"])
     part, cut, _ = jet.partition_big(cfg, chk["graph"], seed=1)
-    chk["thread"].join()
-    o = chk["out"]
-    return {"graph": "R-MAT 2^%d, edge factor 8, k = 256, 2-hop, imbalance 1.10, seed 1" % chk["scale"],
-            "n": chk["graph"].n, "undirected_edges": chk["graph"].nnz // 2, "gpu_cut": cut, "oracle_cut": o["cut"],
-            "partition_equal": bool(np.array_equal(part.cpu().numpy(), o["part"])) and cut == o["cut"],
-            "oracle_seconds_one_thread": o["seconds"]}
+    chk["proc"].join(timeout=900)
+    out = {"graph": "R-MAT 2^%d, edge factor 8, k = 256, 2-hop, imbalance 1.10, seed 1" % chk["scale"],
+           "n": chk["graph"].n, "undirected_edges": chk["graph"].nnz // 2, "gpu_cut": cut}
+    try:
+        meta = json.load(open(chk["base"] + "_meta.json"))
+        opart = np.load(chk["base"] + "_part.npy")
+        out.update(oracle_cut=meta["cut"], oracle_seconds_one_thread=meta["seconds"],
+                   partition_equal=bool(np.array_equal(part.cpu().numpy(), opart)) and cut == meta["cut"])
+    except Exception as e:  # the child did not finish
+        if chk["proc"].is_alive():
+            chk["proc"].terminate()
+        out.update(partition_equal=None, error="oracle run did not finish: %s" % e)
+    shutil.rmtree(chk["dir"], ignore_errors=True)
+    return out
 
 
 def check_full_size_fixture(g, part, cut):

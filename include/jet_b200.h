@@ -264,6 +264,16 @@ int jet_device_ok(void);
  * there); their algorithmic bytes come from device-side counts of that
  * iteration.  jet_prof_read fills ms[13], bytes[13], launches[13]. */
 int jet_prof_enable(int on);
+/* Phase clocks of the persistent level loops (one CTA, cluster, cooperative
+ * grid): with on = 1 a device buffer is cleared and the loops add, per
+ * phase, the SM clock cycles their first thread spent and the number of
+ * times the phase ran; on = 0 copies out[6 * 24] and stops.  Layout:
+ * driver d (0 one CTA, 1 cluster, 2 cooperative) at out[48 d]: cycles of
+ * phases 0-23, then their counts.  Phases: 0 LP select, 1 afterburner,
+ * 2 hub afterburner, 3 rebalance prep, 4 rebalance select, 5 bucket scan,
+ * 6 candidate sort, 7 eviction, 8 strong tail, 9 apply, 10 update subtract,
+ * 11 update add + mark, 12 row rebuild, 13 cut change, 14 control, 15 copy. */
+int jet_prof_phases(int on, uint64_t* out);
 int jet_prof_read(double* ms, double* bytes, int64_t* launches);
 
 /* Number of CUDA kernels this library has launched in this process. */

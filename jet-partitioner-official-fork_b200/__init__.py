@@ -58,8 +58,25 @@ EXPORTED_SYMBOLS = [
     "jet_set_refine_drivers", "jet_partition_batch", "jet_server_create", "jet_server_submit", "jet_server_wait",
     "jet_server_footprint", "jet_server_stats_get", "jet_server_destroy", "jet_refine_hierarchy",
     "jet_device_alloc", "jet_device_free", "jet_copy", "jet_read_metis", "jet_free_host",
-    "jet_test_inject_metis_failures", "jet_test_grid_barrier", "jet_test_table_overflow",
+    "jet_test_inject_metis_failures", "jet_test_grid_barrier", "jet_test_table_overflow", "jet_prof_phases",
 ]
+
+PHASES = ["lp_select", "afterburn", "afterburn_hub", "reb_prep", "reb_select", "bucket_scan", "cand_sort", "evict",
+          "strong_tail", "apply", "update_sub", "update_add", "rebuild", "cut", "control", "copy"]
+
+
+def prof_phases(on: bool):
+    """Phase clocks of the persistent level loops: prof_phases(True) starts,
+    prof_phases(False) returns {driver: {phase: (cycles, count)}}."""
+    out = (ctypes.c_uint64 * (6 * 24))()
+    _check(load().jet_prof_phases(int(on), out))
+    if on:
+        return None
+    res = {}
+    for d, nm in enumerate(["cta", "cluster", "coop"]):
+        res[nm] = {p: (int(out[48 * d + i]), int(out[48 * d + 24 + i])) for i, p in enumerate(PHASES)
+                   if out[48 * d + 24 + i]}
+    return res
 
 # level-loop drivers (jet_set_refine_drivers)
 DRIVER_CTA, DRIVER_COOP, DRIVER_GRAPH, DRIVER_CLUSTER, DRIVER_CTA_SMEM, DRIVER_ALL = 1, 2, 4, 8, 16, 31

@@ -462,6 +462,8 @@ int prof_begin(cudaStream_t s);
 void prof_end(int h, ProfKernel k, double bytes, cudaStream_t s);
 void prof_add_bytes(int h, double bytes);
 bool prof_active();
+// Device buffer of the persistent level loops' phase clocks (jet_prof_phases), or null.
+unsigned long long* phase_clk_ptr();
 void prof_collect();  // after a stream sync: folds event pairs into the slots
 
 }  // namespace jetb

@@ -239,6 +239,7 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
     const O n = a.g.n;
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl_begin_logic(c);
     if (!level_sync<CL>(cs.bar, err)) return;
+    PhaseClock pc(a.pclk, CL ? 2 * PHASE_SLOTS : 4 * PHASE_SLOTS, blockIdx.x == 0 && threadIdx.x == 0);
     int iters = 0;
     while (true) {
         const int more = ((volatile Ctl<W>*)c)->more;
@@ -249,6 +250,7 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             d_lp_select_warp<O, E, W>(a, li.warp_list, li.n_warp);
             d_lp_select_warp<O, E, W>(a, li.hub_list, li.n_hub);
             if (!level_sync<CL>(cs.bar, err)) return;
+            pc.mark(PH_LP_SELECT);
             switch (li.group) {
                 case 4: d_afterburn<4, O, E, W>(a); break;
                 case 8: d_afterburn<8, O, E, W>(a); break;
@@ -256,8 +258,10 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
                 default: d_afterburn<32, O, E, W>(a); break;
             }
             if (!level_sync<CL>(cs.bar, err)) return;
+            pc.mark(PH_AFTERBURN);
             d_afterburn_hub<O, E, W>(a);
             if (!level_sync<CL>(cs.bar, err)) return;
+            pc.mark(PH_AFTERBURN_HUB);
         } else {
             RebArgs<O, W>& rb = mode == MODE_WEAK ? rbw : rbs;
             coop_zero<O, E, W>(rb.buckets, (int64_t)rb.t_minibuckets + 1 + rb.width);
@@ -267,6 +271,7 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
                 else d_strong_prep<O, E, W>(a, rb);
             }
             if (!level_sync<CL>(cs.bar, err)) return;
+            pc.mark(PH_REB_PREP);
             if (mode == MODE_WEAK) {
                 d_weak_select_thread<O, E, W>(a, rb);
                 d_weak_select_warp<O, E, W>(a, rb, li.warp_list, li.n_warp);
@@ -277,12 +282,15 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
                 d_strong_score_warp<O, E, W>(a, rb, li.hub_list, li.n_hub);
             }
             if (!level_sync<CL>(cs.bar, err)) return;
+            pc.mark(PH_REB_SELECT);
             bool ok = mode == MODE_WEAK ? coop_reb_tail<CL, false, O, E, W>(a, rb, cs, bits) : coop_reb_tail<CL, true, O, E, W>(a, rb, cs, bits);
             if (!ok) return;
+            pc.mark(PH_REB_EVICT);
         }
         // perform_moves (src/jet_refiner.hpp:905-955)
         d_apply_moves<O, E, W>(a, 0);
         if (!level_sync<CL>(cs.bar, err)) return;
+        pc.mark(PH_APPLY);
         switch (li.group) {
             case 4: d_update_small<4, false, O, E, W>(a); break;
             case 8: d_update_small<8, false, O, E, W>(a); break;
@@ -291,6 +299,7 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
         }
         d_update_small_hub<false, O, E, W>(a);
         if (!level_sync<CL>(cs.bar, err)) return;
+        pc.mark(PH_UPDATE_SUB);
         switch (li.group) {
             case 4: d_update_small<4, true, O, E, W>(a); d_mark_neighbors<4, O, E, W>(a); break;
             case 8: d_update_small<8, true, O, E, W>(a); d_mark_neighbors<8, O, E, W>(a); break;
@@ -300,6 +309,7 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
         d_update_small_hub<true, O, E, W>(a);
         d_mark_neighbors_hub<O, E, W>(a);
         if (!level_sync<CL>(cs.bar, err)) return;
+        pc.mark(PH_UPDATE_ADD);
         if (a.dev->large) {
             // update_large: queue the marked rows (one coalesced pass), then
             // rebuild them one warp per row
@@ -313,8 +323,10 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             d_conn_warp<O, E, W>(a, cs.marked, (O)((volatile GridBar*)cs.bar)->nmarked, 1, nullptr);
             if (!level_sync<CL>(cs.bar, err)) return;
         }
+        pc.mark(PH_REBUILD);
         d_cut_after<O, E, W>(a);
         if (!level_sync<CL>(cs.bar, err)) return;
+        pc.mark(PH_CUT);
         if (blockIdx.x == 0) {
             W mx = block_max_sizes<W>(a.sizes, a.k);
             if (threadIdx.x == 0) {
@@ -324,13 +336,16 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             }
         }
         if (!level_sync<CL>(cs.bar, err)) return;
+        pc.mark(PH_CTL);
         if (((volatile Ctl<W>*)c)->copy) {
             for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
                 best_part[i] = a.part[i];
             for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.k; p += gridDim.x * blockDim.x) sizes_best[p] = a.sizes[p];
         }
         if (!level_sync<CL>(cs.bar, err)) return;
+        pc.mark(PH_COPY);
     }
+    pc.flush();
 }
 
 }  // namespace jetb

@@ -47,10 +47,11 @@ __device__ __forceinline__ void block_scan_global(const T* in, T* out, int64_t n
 // scores: the block-level form of sort_candidates + k_evict_sorted (+ the
 // strong rebalance's cookie cutter and destination draws).
 template <bool STRONG, class O, class E, class W>
-__device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb, uint64_t* keys, int P) {
+__device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb, uint64_t* keys, int P, PhaseClock& pc) {
     __shared__ W sw[32];
     const O n = a.g.n;
     block_scan_global<W>(rb.buckets, rb.boff, (int64_t)rb.t_minibuckets + 1);
+    pc.mark(PH_REB_SCAN);
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
         uint64_t key = ~0ull;
         if (i < n) {
@@ -62,6 +63,7 @@ __device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb,
     if (STRONG) for (int p = threadIdx.x; p < a.k; p += blockDim.x) rb.evict_adjust[p] = 0;
     __syncthreads();
     block_sort_keys<uint64_t>(keys, P);
+    pc.mark(PH_REB_SORT);
     W carry = 0;
     for (int base = 0; base < (int)n; base += blockDim.x) {
         int q = base + threadIdx.x;
@@ -90,6 +92,7 @@ __device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb,
         carry += tot;
     }
     __syncthreads();
+    pc.mark(PH_REB_EVICT);
     if (STRONG) {
         d_cookie<O, E, W>(a, rb);
         __syncthreads();
@@ -97,6 +100,7 @@ __device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb,
         __syncthreads();
         d_strong_redraw<O, E, W>(a, rb);
         __syncthreads();
+        pc.mark(PH_STRONG_TAIL);
     }
 }
 
@@ -170,6 +174,7 @@ k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, 
         s_more = c->more;
     }
     __syncthreads();
+    PhaseClock pc(a.pclk, 0, threadIdx.x == 0);
     int iters = 0;
     while (s_more) {
         const int mode = s_mode;
@@ -178,6 +183,7 @@ k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, 
             d_lp_select_warp<O, E, W>(a, li.warp_list, li.n_warp);
             d_lp_select_warp<O, E, W>(a, li.hub_list, li.n_hub);
             __syncthreads();
+            pc.mark(PH_LP_SELECT);
             switch (li.group) {
                 case 4: d_afterburn<4, O, E, W>(a); break;
                 case 8: d_afterburn<8, O, E, W>(a); break;
@@ -185,30 +191,37 @@ k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, 
                 default: d_afterburn<32, O, E, W>(a); break;
             }
             __syncthreads();
+            pc.mark(PH_AFTERBURN);
             d_afterburn_hub<O, E, W>(a);
             __syncthreads();
+            pc.mark(PH_AFTERBURN_HUB);
         } else if (mode == MODE_WEAK) {
             cta_zero_buckets<O, E, W>(rbw);
             d_weak_prep<O, E, W>(a, rbw);
             __syncthreads();
+            pc.mark(PH_REB_PREP);
             d_weak_select_thread<O, E, W>(a, rbw);
             d_weak_select_warp<O, E, W>(a, rbw, li.warp_list, li.n_warp);
             d_weak_select_warp<O, E, W>(a, rbw, li.hub_list, li.n_hub);
             __syncthreads();
-            d_reb_tail<false, O, E, W>(a, rbw, keys, P);
+            pc.mark(PH_REB_SELECT);
+            d_reb_tail<false, O, E, W>(a, rbw, keys, P, pc);
         } else {
             cta_zero_buckets<O, E, W>(rbs);
             d_strong_prep<O, E, W>(a, rbs);
             __syncthreads();
+            pc.mark(PH_REB_PREP);
             d_strong_score_thread<O, E, W>(a, rbs);
             d_strong_score_warp<O, E, W>(a, rbs, li.warp_list, li.n_warp);
             d_strong_score_warp<O, E, W>(a, rbs, li.hub_list, li.n_hub);
             __syncthreads();
-            d_reb_tail<true, O, E, W>(a, rbs, keys, P);
+            pc.mark(PH_REB_SELECT);
+            d_reb_tail<true, O, E, W>(a, rbs, keys, P, pc);
         }
         // perform_moves (src/jet_refiner.hpp:905-955)
         d_apply_moves<O, E, W>(a, 0);
         __syncthreads();
+        pc.mark(PH_APPLY);
         switch (li.group) {
             case 4: d_update_small<4, false, O, E, W>(a); break;
             case 8: d_update_small<8, false, O, E, W>(a); break;
@@ -217,6 +230,7 @@ k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, 
         }
         d_update_small_hub<false, O, E, W>(a);
         __syncthreads();
+        pc.mark(PH_UPDATE_SUB);
         switch (li.group) {
             case 4: d_update_small<4, true, O, E, W>(a); d_mark_neighbors<4, O, E, W>(a); break;
             case 8: d_update_small<8, true, O, E, W>(a); d_mark_neighbors<8, O, E, W>(a); break;
@@ -226,10 +240,13 @@ k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, 
         d_update_small_hub<true, O, E, W>(a);
         d_mark_neighbors_hub<O, E, W>(a);
         __syncthreads();
+        pc.mark(PH_UPDATE_ADD);
         d_conn_warp<O, E, W>(a, nullptr, n, 1, &a.dev->large);  // update_large: rebuild marked rows
         __syncthreads();
+        pc.mark(PH_REBUILD);
         d_cut_after<O, E, W>(a);
         __syncthreads();
+        pc.mark(PH_CUT);
         W mx = block_max_sizes<W>(a.sizes, a.k);
         if (threadIdx.x == 0) {
             ctl_end_logic<O, W>(c, a.dev, mx);
@@ -239,12 +256,15 @@ k_level_cta(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O, 
             if (c->more && iters >= max_iters) atomicOr(&a.dev->err, ERRF_SPIN);
         }
         __syncthreads();
+        pc.mark(PH_CTL);
         if (s_copy) {
             for (int64_t i = threadIdx.x; i < n; i += blockDim.x) best_part[i] = a.part[i];
             for (int p = threadIdx.x; p < a.k; p += blockDim.x) sizes_best[p] = a.sizes[p];
         }
         __syncthreads();
+        pc.mark(PH_COPY);
     }
+    pc.flush();
     // the host reads the control state and the error flags after the level
     if (threadIdx.x == 0) {
         if (plan.ctl != NO_SMEM) *c_global = *c;

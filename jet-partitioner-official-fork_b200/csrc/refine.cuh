@@ -94,6 +94,45 @@ struct RefArgs {
     RefDev<O, W>* dev;
     const double* filter;  // LP filter ratio, read on the device (it changes per iteration with ultra settings)
     int narrow;            // every row's summed edge weight fits in 32 bits (see acc_add)
+    unsigned long long* pclk;  // per-phase clock totals of the persistent level loops, or null (jet_prof_phases)
+};
+
+// Per-phase clock totals of a persistent level loop, kept by one thread in
+// local memory and added to a.pclk when the loop ends (phase-time profiling
+// only; nothing is recorded without a.pclk).  Slots [base + id] hold cycles,
+// [base + PHASE_SLOTS + id] the number of times the phase ran.
+static constexpr int PHASE_SLOTS = 24;
+enum PhaseId : int {
+    PH_LP_SELECT = 0, PH_AFTERBURN, PH_AFTERBURN_HUB, PH_REB_PREP, PH_REB_SELECT, PH_REB_SCAN, PH_REB_SORT, PH_REB_EVICT,
+    PH_STRONG_TAIL, PH_APPLY, PH_UPDATE_SUB, PH_UPDATE_ADD, PH_REBUILD, PH_CUT, PH_CTL, PH_COPY, PH_COUNT
+};
+struct PhaseClock {
+    unsigned long long* out;
+    int base;
+    bool on;
+    long long last;
+    unsigned long long cyc[PH_COUNT];
+    unsigned cnt[PH_COUNT];
+    __device__ PhaseClock(unsigned long long* p, int b, bool owner) : out(p), base(b), on(p != nullptr && owner), last(0) {
+        if (on) {
+            for (int i = 0; i < PH_COUNT; i++) { cyc[i] = 0; cnt[i] = 0; }
+            last = clock64();
+        }
+    }
+    __device__ __forceinline__ void mark(int id) {
+        if (!on) return;
+        long long t = clock64();
+        cyc[id] += (unsigned long long)(t - last);
+        cnt[id]++;
+        last = t;
+    }
+    __device__ void flush() {
+        if (!on) return;
+        for (int i = 0; i < PH_COUNT; i++) {
+            atomicAdd(&out[base + i], cyc[i]);
+            atomicAdd(&out[base + PHASE_SLOTS + i], (unsigned long long)cnt[i]);
+        }
+    }
 };
 
 
@@ -1267,9 +1306,16 @@ __device__ __forceinline__ void d_strong_first(RefArgs<O, E, W> a, RebArgs<O, W>
         part_t pv = a.part[v];
         W sc = rb.score[v] + rb.boff[rb.bid[v]] - rb.evict_adjust[pv];
         W w = a.g.vw[v];
-        int p = 0;
-        while (p <= a.k && rb.evict_start[p] <= sc) p++;
-        p--;
+        // the chunk holding position sc: the last p with evict_start[p] <= sc
+        // (evict_start is a prefix of non-negative capacities, so a binary
+        // search finds what a scan from p = 0 would)
+        int lo = 0, hi = a.k + 1;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (rb.evict_start[mid] <= sc) lo = mid + 1;
+            else hi = mid;
+        }
+        int p = lo - 1;
         part_t dest = pv;
         if (p < 0) atomicOr(&a.dev->err, ERRF_SPIN);  // positions are never negative
         else if (p < a.k) {

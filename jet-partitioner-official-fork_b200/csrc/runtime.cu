@@ -393,6 +393,9 @@ int prof_begin(cudaStream_t s) {
     return h;
 }
 
+static unsigned long long* g_pclk = nullptr;  // phase clocks of the persistent level loops
+unsigned long long* phase_clk_ptr() { return g_pclk; }
+
 bool prof_active() {
     std::lock_guard<std::recursive_mutex> lk(g_prof_mu);
     return g_prof.on && !capturing();
@@ -510,6 +513,21 @@ int jet_project(int tier, int64_t n_fine, const void* map, const int32_t* coarse
 }
 
 int64_t jet_launch_count(void) { return g_launches.load(); }
+
+int jet_prof_phases(int on, uint64_t* out) {
+    const size_t bytes = sizeof(unsigned long long) * 6 * PHASE_SLOTS;
+    if (on) {
+        if (!g_pclk && cudaMalloc(&g_pclk, bytes) != cudaSuccess) { g_pclk = nullptr; return JET_ERR_OOM; }
+        return cudaMemset(g_pclk, 0, bytes) == cudaSuccess ? JET_OK : JET_ERR_CUDA;
+    }
+    if (!g_pclk) return JET_OK;
+    cudaDeviceSynchronize();
+    int rc = JET_OK;
+    if (out && cudaMemcpy(out, g_pclk, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) rc = JET_ERR_CUDA;
+    cudaFree(g_pclk);
+    g_pclk = nullptr;
+    return rc;
+}
 
 int jet_test_inject_metis_failures(int count) { return g_metis_fail.exchange(count < 0 ? 0 : count); }
 

@@ -134,6 +134,7 @@ struct Refiner {
         a.pregain = pregain.p; a.sizes = sizes_curr.p; a.cand = cand.p; a.cand_hub = cand_hub.p; a.moves = moves.p;
         a.moves_hub = moves_hub.p; a.dev = dev.p; a.filter = &ctl.p->filter;
         a.narrow = narrow_state > 0 ? 1 : 0;
+        a.pclk = phase_clk_ptr();
         return a;
     }
 
@@ -271,8 +272,10 @@ struct Refiner {
         prof_end(h, PK_CONN_BUILD, bytes, s);
         fill<part_t>(dest_cache.p, L.n, NULL_PART, s);
         JET_CUDA(cudaMemsetAsync(lock.p, 0, L.n, s));
+        last_slots = (int64_t)C;
         return (int64_t)C;
     }
+    int64_t last_slots = 0;  // table slots of the level init_conn built last
 
     // Profiling-pass handles of the current iteration's class brackets.
     int ph[PK_COUNT];
@@ -721,10 +724,8 @@ struct Refiner {
         // maximum, so concurrent callers with different sizes cannot race
         const size_t smax = max_dynamic_smem((const void*)k_level_cta<O, E, W>);
         JET_CUDA(cudaFuncSetAttribute(k_level_cta<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
-        // the level's table slots: the capacities' total (coff[n]) as init_conn left it
-        JET_CUDA(cudaMemcpyAsync(e.hscal, coff.p + L.n, sizeof(E), cudaMemcpyDeviceToHost, s));
-        e.sync();
-        const int64_t nslots = (int64_t)*(E*)e.hscal;
+        // the level's table slots, as init_conn counted them
+        const int64_t nslots = last_slots;
         const int64_t nbuckets = (int64_t)rbw.t_minibuckets + 1 + rbw.width;
         CtaSmemPlan plan = plan_cta_smem<O, W>((int64_t)L.n, nslots, nbuckets, k, scratch, smax, cta_smem_resident());
         k_level_cta<O, E, W><<<1, CTA_THREADS, plan.total, s>>>(args(L), li, rbw, rbs, ctl.p, best_part, sizes_best.p, P,

@@ -211,7 +211,7 @@ def rgg(n: int, mean_degree: float = 10.0, seed: int = 1, weighted: bool = True,
     cx = (pts[:, 0] * cells).long().clamp_(max=cells - 1)
     cy = (pts[:, 1] * cells).long().clamp_(max=cells - 1)
     cell = cy * cells + cx
-    order = torch.argsort(cell)
+    order = torch.argsort(cell, stable=True)  # stable: the same edge order (and weights) on every device
     cell_sorted = cell[order]
     starts = torch.searchsorted(cell_sorted, torch.arange(cells * cells + 1, device=device))
     us, vs = [], []
