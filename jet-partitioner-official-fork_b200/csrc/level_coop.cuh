@@ -180,46 +180,6 @@ struct CoopScratch {
     O* marked;           // rows to rebuild after a large move set (n)
 };
 
-static constexpr int COOP_SMALL_CAP = 4096;
-
-// Gathers the rebalance candidates (bid >= 0) in vertex order into
-// (cs.sk0 = bucket, cs.sv0 = vertex); every block learns their number in
-// *count.  Blocks own contiguous vertex ranges, in block order.
-template <bool CL, class O, class E, class W>
-__device__ __forceinline__ bool grid_gather_candidates(const RebArgs<O, W>& rb, int64_t n, CoopScratch<O, E, W>& cs,
-                                                       int64_t* count, int* err) {
-    __shared__ uint32_t su[32];
-    __shared__ int64_t s_off, s_total;
-    const int64_t chunk = ceil_div<int64_t>(n, (int64_t)gridDim.x);
-    const int64_t lo = chunk * blockIdx.x, hi = lo + chunk < n ? lo + chunk : n;
-    uint32_t c = 0;
-    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) c += rb.bid[i] >= 0;
-    uint32_t tot;
-    block_exclusive_scan<uint32_t>(c, su, tot);
-    if (threadIdx.x == 0) cs.hist[blockIdx.x] = tot;  // the radix histogram space is free here
-    if (!level_sync<CL>(cs.bar, err)) return false;
-    {
-        // this block's offset and the total, one earlier block per thread
-        uint32_t v = threadIdx.x < gridDim.x ? ld_cg(&cs.hist[threadIdx.x]) : 0u;
-        uint32_t all;
-        uint32_t before = block_exclusive_scan<uint32_t>(v, su, all);
-        if (threadIdx.x == blockIdx.x) s_off = before;
-        if (threadIdx.x == 0) s_total = all;
-        __syncthreads();
-    }
-    int64_t carry = s_off;
-    for (int64_t base = lo; base < hi; base += blockDim.x) {
-        int64_t i = base + threadIdx.x;
-        O b = i < hi ? rb.bid[i] : (O)-1;
-        uint32_t f = b >= 0 ? 1u : 0u, t2;
-        uint32_t ex = block_exclusive_scan<uint32_t>(f, su, t2);
-        if (f) { cs.sk0[carry + ex] = (uint32_t)b; cs.sv0[carry + ex] = (O)i; }
-        carry += t2;
-    }
-    *count = s_total;
-    return level_sync<CL>(cs.bar, err);
-}
-
 // Rebalance tail over the grid (sort_candidates + k_evict_sorted [+ strong]).
 template <bool CL, bool STRONG, class O, class E, class W>
 __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>& rb, CoopScratch<O, E, W>& cs, int bits) {
@@ -227,34 +187,6 @@ __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>
     if (!grid_scan<CL, W>(GetArray<W>{rb.buckets}, (int64_t)rb.t_minibuckets + 1, rb.boff, cs.wsum, cs.bar, err)) return false;
     const int64_t n = a.g.n;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    {
-        // few candidates: one block sorts and evicts them (the others wait)
-        int64_t ncand = 0;
-        if (!grid_gather_candidates<CL, O, E, W>(rb, n, cs, &ncand, err)) return false;
-        if (ncand <= COOP_SMALL_CAP) {
-            if (STRONG) {
-                for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.k; p += gridDim.x * blockDim.x) rb.evict_adjust[p] = 0;
-                if (!level_sync<CL>(cs.bar, err)) return false;
-            }
-            if (blockIdx.x == 0) {
-                uint64_t* keys = (uint64_t*)smem_raw;
-                for (int q = threadIdx.x; q < (int)ncand; q += blockDim.x)
-                    keys[q] = ((uint64_t)ld_cg(&cs.sk0[q]) << 32) | (uint32_t)ld_cg(&cs.sv0[q]);
-                __syncthreads();
-                block_reb_small<STRONG, COOP_SMALL_CAP, O, E, W>(a, rb, keys, (int)ncand, nullptr);
-            }
-            if (!level_sync<CL>(cs.bar, err)) return false;
-            if (STRONG) {
-                if (blockIdx.x == 0) d_cookie<O, E, W>(a, rb);
-                if (!level_sync<CL>(cs.bar, err)) return false;
-                d_strong_first<O, E, W>(a, rb);
-                if (!level_sync<CL>(cs.bar, err)) return false;
-                if (blockIdx.x == 0) d_strong_redraw<O, E, W>(a, rb);
-                if (!level_sync<CL>(cs.bar, err)) return false;
-            }
-            return true;
-        }
-    }
     uint32_t(*cnt)[RS_BINS] = (uint32_t(*)[RS_BINS])smem_raw;  // 32 x 256 counters (dynamic shared memory)
     // stable sort of (bucket id, vertex) pairs
     int passes = (bits + 7) / 8;

@@ -43,143 +43,15 @@ __device__ __forceinline__ void block_scan_global(const T* in, T* out, int64_t n
     __syncthreads();
 }
 
-// ---------------------------------------------------------------- small candidate sets
-// A rebalance iteration orders its candidates by (bucket, vertex id) to give
-// each the weight of the earlier candidates in its bucket -- the score the
-// reference reads from its per-bucket atomic fetch-add in vertex order
-// (src/jet_refiner.hpp:476, :640).  The candidates are usually a small part of
-// the level (the vertices of the few oversized parts), so when at most CAP of
-// them exist one block sorts just them: the list is gathered in vertex order,
-// then a stable LSD radix sort over 4-bit digits of the bucket id keeps that
-// order inside every bucket.  Keys are (bucket << 32 | vertex).
-template <int CAP>
-constexpr size_t small_sort_smem() { return (size_t)CAP * 16 + (size_t)16 * CTA_THREADS * sizeof(uint16_t) + 64; }
-
-__device__ __forceinline__ int key_bits(uint32_t maxval) { return maxval ? 32 - __clz(maxval) : 1; }
-
-// Sorts keys[0..P) (P <= CAP) stably by their upper 32 bits, using tmp and
-// cnt (16 x blockDim 16-bit counters); returns the buffer holding the result.
-template <int CAP>
-__device__ __forceinline__ uint64_t* block_sort_by_bucket(uint64_t* keys, uint64_t* tmp, uint16_t* cnt, int P, int bits) {
-    __shared__ uint32_t sw[32];
-    const int t = threadIdx.x, nt = blockDim.x;
-    const int items = (P + nt - 1) / nt;  // each thread owns `items` consecutive keys
-    for (int shift = 32; shift < 32 + bits; shift += 4) {
-        uint32_t c[16];
-        for (int d = 0; d < 16; d++) c[d] = 0;
-        for (int j = 0; j < items; j++) {
-            int idx = t * items + j;
-            if (idx < P) c[(int)((keys[idx] >> shift) & 15u)]++;
-        }
-        for (int d = 0; d < 16; d++) cnt[d * nt + t] = (uint16_t)c[d];
-        __syncthreads();
-        // exclusive scan of the counters in (digit, thread) order: thread t
-        // takes 16 consecutive entries
-        uint32_t run = 0;
-        for (int q = 0; q < 16; q++) { uint32_t v = cnt[t * 16 + q]; c[q] = run; run += v; }
-        uint32_t tot;
-        uint32_t ex = block_exclusive_scan<uint32_t>(run, sw, tot);
-        for (int q = 0; q < 16; q++) cnt[t * 16 + q] = (uint16_t)(ex + c[q]);
-        __syncthreads();
-        for (int d = 0; d < 16; d++) c[d] = cnt[d * nt + t];
-        for (int j = 0; j < items; j++) {
-            int idx = t * items + j;
-            if (idx < P) {
-                uint64_t k = keys[idx];
-                tmp[c[(int)((k >> shift) & 15u)]++] = k;
-            }
-        }
-        __syncthreads();
-        uint64_t* sw2 = keys; keys = tmp; tmp = sw2;
-    }
-    return keys;
-}
-
-// Eviction decisions for the P candidates in keys[0..P) (vertex order): the
-// block form of sort_candidates + k_evict_sorted for a small candidate set.
-template <bool ADJUST, int CAP, class O, class E, class W>
-__device__ __forceinline__ void block_reb_small(RefArgs<O, E, W>& a, RebArgs<O, W>& rb, uint64_t* keys, int P,
-                                                unsigned char* scratch) {
-    __shared__ W sw[32];
-    uint64_t* tmp = keys + CAP;
-    uint16_t* cnt = (uint16_t*)(tmp + CAP);
-    uint64_t* sorted = block_sort_by_bucket<CAP>(keys, tmp, cnt, P, key_bits(rb.none_key));
-    (void)scratch;
-    const int t = threadIdx.x, items = (P + (int)blockDim.x - 1) / (int)blockDim.x;
-    W wsum = 0;
-    for (int j = 0; j < items; j++) {
-        int idx = t * items + j;
-        if (idx < P) wsum += a.g.vw[(O)(uint32_t)(sorted[idx] & 0xffffffffu)];
-    }
-    W tot;
-    W run = block_exclusive_scan<W>(wsum, sw, tot);
-    for (int j = 0; j < items; j++) {
-        int idx = t * items + j;
-        if (idx >= P) break;
-        uint64_t key = sorted[idx];
-        O b = (O)(uint32_t)(key >> 32);
-        O i = (O)(uint32_t)(key & 0xffffffffu);
-        W w = a.g.vw[i];
-        part_t p = a.part[i];
-        O begin = (O)p * rb.width;
-        W within = run - bucket_start<O, W>(rb, b);
-        if (ADJUST) rb.score[i] = within;
-        W score = within + bucket_pos<O, W>(rb, b) - bucket_pos<O, W>(rb, begin);
-        W limit = a.sizes[p] - rb.size_max;
-        if (score < limit) {
-            if (ADJUST && score + w >= limit) rb.evict_adjust[p] = score + w;
-            O s = atomic_add(&a.dev->nmoves, (O)1);
-            a.moves[s] = i;
-        }
-        run += w;
-    }
-    __syncthreads();
-}
-
 // Bucket offsets, candidates in (bucket, vertex) order and their eviction
 // scores: the block-level form of sort_candidates + k_evict_sorted (+ the
 // strong rebalance's cookie cutter and destination draws).
-static constexpr int CTA_SMALL_CAP = 2048;
-
 template <bool STRONG, class O, class E, class W>
 __device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb, uint64_t* keys, int P, PhaseClock& pc) {
     __shared__ W sw[32];
-    __shared__ uint32_t su[32];
-    __shared__ int s_ncand;
     const O n = a.g.n;
     block_scan_global<W>(rb.buckets, rb.boff, (int64_t)rb.t_minibuckets + 1);
     pc.mark(PH_REB_SCAN);
-    // the candidates in vertex order, while they fit the small-set sort
-    {
-        uint32_t carry = 0;
-        bool fits = true;
-        for (int base = 0; base < (int)n; base += blockDim.x) {
-            int i = base + threadIdx.x;
-            O b = i < (int)n ? rb.bid[i] : (O)-1;
-            uint32_t f = b >= 0 ? 1u : 0u, tot;
-            uint32_t ex = block_exclusive_scan<uint32_t>(f, su, tot);
-            if (f && carry + ex < (uint32_t)CTA_SMALL_CAP) keys[carry + ex] = ((uint64_t)(uint32_t)b << 32) | (uint32_t)i;
-            carry += tot;
-            if (carry > (uint32_t)CTA_SMALL_CAP) { fits = false; break; }
-        }
-        if (threadIdx.x == 0) s_ncand = fits ? (int)carry : -1;
-        if (STRONG) for (int p = threadIdx.x; p < a.k; p += blockDim.x) rb.evict_adjust[p] = 0;
-        __syncthreads();
-    }
-    if (s_ncand >= 0) {
-        block_reb_small<STRONG, CTA_SMALL_CAP, O, E, W>(a, rb, keys, s_ncand, nullptr);
-        pc.mark(PH_REB_SORT);
-        if (STRONG) {
-            d_cookie<O, E, W>(a, rb);
-            __syncthreads();
-            d_strong_first<O, E, W>(a, rb);
-            __syncthreads();
-            d_strong_redraw<O, E, W>(a, rb);
-            __syncthreads();
-            pc.mark(PH_STRONG_TAIL);
-        }
-        return;
-    }
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
         uint64_t key = ~0ull;
         if (i < n) {
@@ -446,7 +318,7 @@ inline CtaSmemPlan plan_cta_smem(int64_t n, int64_t nslots, int64_t nbuckets, in
 
 template <class O, class W>
 constexpr size_t level_cta_smem(int P, int k) {
-    size_t sort_b = (size_t)P * 8 > small_sort_smem<CTA_SMALL_CAP>() ? (size_t)P * 8 : small_sort_smem<CTA_SMALL_CAP>();
+    size_t sort_b = (size_t)P * 8;
     size_t conn_b = (((size_t)(CTA_THREADS / 32) * k * sizeof(part_t) + 15) & ~(size_t)15) + (size_t)(CTA_THREADS / 32) * k * sizeof(W);
     return sort_b > conn_b ? sort_b : conn_b;
 }

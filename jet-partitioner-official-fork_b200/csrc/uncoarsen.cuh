@@ -742,9 +742,7 @@ struct Refiner {
         size_t nw = CTA_THREADS / 32;
         size_t conn = ((nw * kw * sizeof(part_t) + 15) & ~(size_t)15) + nw * kw * sizeof(W);
         size_t rs = (size_t)32 * RS_BINS * sizeof(uint32_t);
-        size_t small = small_sort_smem<COOP_SMALL_CAP>();
-        size_t m = conn > rs ? conn : rs;
-        return (m > small ? m : small) + 64;
+        return (conn > rs ? conn : rs) + 64;
     }
     size_t coop_static_smem() const {
         static size_t bytes = [] {
