@@ -445,10 +445,13 @@ def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None, cpu_cores=0):
     t_plain = max_over_ranks(time.perf_counter() - t0, ws, dist, dev)
     if ws > 1:
         dist.barrier()
+    m0 = jet.metis_call_stats()
     t0 = time.perf_counter()
     res = jet.partition_batch(cfgs, gs, seeds, workers=workers)
     torch.cuda.synchronize()
     t_batch = max_over_ranks(time.perf_counter() - t0, ws, dist, dev)
+    m1 = jet.metis_call_stats()
+    metis = {k: m1[k] - m0[k] if isinstance(m1[k], int) and not isinstance(m1[k], bool) else m1[k] for k in m1}
     equal = max_over_ranks(0.0 if all(r[1] == p for r, p in zip(res, plain)) else 1.0, ws, dist, dev) == 0.0
     lat = sorted(r[2] for r in res) or [0.0]
     edges = sum(g.nnz for g in gs) // 2
@@ -459,7 +462,7 @@ def run_batched(jet, dev, count, workers, ws=1, rank=0, dist=None, cpu_cores=0):
         cpu_cuts = cpu.pop("cuts")
         ratios = [r[1] / max(c, 1) for r, c in zip(res, cpu_cuts) if c is not None]
         cpu["cut_ratio_median"] = statistics.median(ratios) if ratios else None
-    return {"cpu_baseline": cpu, "graphs": count, "graphs_this_rank": len(mine), "workers": workers,
+    return {"cpu_baseline": cpu, "metis_calls_batched": metis, "graphs": count, "graphs_this_rank": len(mine), "workers": workers,
             "sum_vertices_this_rank": sum(g.n for g in gs), "undirected_edges_this_rank": edges,
             "plain_graphs_per_s": count / t_plain, "batched_graphs_per_s": count / t_batch,
             "speedup": t_plain / t_batch, "equal_cut": equal,
@@ -830,9 +833,6 @@ def main():
     cpu_cores = 0
     if ws == 1 and not args.no_cpu_baseline:
         cpu_cores = _oracle_mods()[1].concurrency("host")
-    chk = None
-    if args.powerlaw_scale > 0 and args.check_scale > 0 and rank == 0:
-        chk = start_oracle_check(jet, dev, args.check_scale)
     batched = run_batched(jet, dev, args.batched, args.workers, ws, rank, dist, cpu_cores) if args.batched > 0 else None
     stage("batched done")
     serving = None
@@ -840,6 +840,12 @@ def main():
         serving = run_serving(jet, dev, args.serving, args.workers, 120 << 30, nmax=args.serving_nmax,
                               pool=args.serving_pool, rates=[float(x) for x in args.serving_rates.split(",") if x])
     stage("serving done")
+    # the oracle's partition of a smaller power-law graph runs in a child
+    # process from here on, beside the power-law leg's GPU work (it would take
+    # host cores from the batched and served legs)
+    chk = None
+    if args.powerlaw_scale > 0 and args.check_scale > 0 and rank == 0:
+        chk = start_oracle_check(jet, dev, args.check_scale)
     powerlaw = None
     if args.powerlaw_scale > 0 and rank == 0:
         powerlaw = run_powerlaw(jet, dev, args.powerlaw_scale, cpu_scale=(args.powerlaw_scale - 3) if cpu_cores else 0,

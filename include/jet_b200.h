@@ -294,6 +294,11 @@ int64_t jet_launch_count(void);
  *     connectivity table of `cap` slots (k parts) with the table-build insert;
  *     JET_ERR_OVERFLOW when the probe bound flagged a full table. */
 int jet_test_inject_metis_failures(int count);
+/* Coarsest-graph Metis calls of this process: out[5] = {calls served by helper
+ * processes, helper calls that failed (rerun in-process, the helper
+ * replaced), in-process calls, helpers started, 1 if helpers could not be
+ * started}. */
+int jet_metis_call_stats(int64_t* out);
 int jet_test_grid_barrier(int blocks, int absent_block, int spin_cap_log2, int rounds, int* passed);
 int jet_test_table_overflow(int cap, int k, int nparts, int* claimed);
 

@@ -58,8 +58,16 @@ EXPORTED_SYMBOLS = [
     "jet_set_refine_drivers", "jet_partition_batch", "jet_server_create", "jet_server_submit", "jet_server_wait",
     "jet_server_footprint", "jet_server_stats_get", "jet_server_destroy", "jet_refine_hierarchy",
     "jet_device_alloc", "jet_device_free", "jet_copy", "jet_read_metis", "jet_free_host",
-    "jet_test_inject_metis_failures", "jet_test_grid_barrier", "jet_test_table_overflow", "jet_prof_phases",
+    "jet_test_inject_metis_failures", "jet_test_grid_barrier", "jet_test_table_overflow", "jet_prof_phases", "jet_metis_call_stats",
 ]
+
+
+def metis_call_stats() -> dict:
+    """Where this process's coarsest-graph Metis calls ran (jet_metis_call_stats)."""
+    out = (ctypes.c_int64 * 5)()
+    _check(load().jet_metis_call_stats(out))
+    return dict(helper_calls=out[0], helper_failures=out[1], inprocess_calls=out[2], helpers=out[3],
+                helpers_unavailable=bool(out[4]))
 
 PHASES = ["lp_select", "afterburn", "afterburn_hub", "reb_prep", "reb_select", "bucket_scan", "cand_sort", "evict",
           "strong_tail", "apply", "update_sub", "update_add", "rebuild", "cut", "control", "copy"]

@@ -3,6 +3,7 @@
 // profiling and the tier-generic C entry points.
 #include "api_impl.cuh"
 #include <atomic>
+#include <cerrno>
 #include <chrono>
 #include <condition_variable>
 #include <mutex>
@@ -212,10 +213,12 @@ bool spawn_helper(Helper& h) {
     return true;
 }
 
+// Both retry a transfer that a signal interrupted.
 bool send_all(int fd, const void* p, size_t bytes) {
     const char* c = (const char*)p;
     while (bytes > 0) {
         ssize_t r = send(fd, c, bytes, MSG_NOSIGNAL);
+        if (r < 0 && errno == EINTR) continue;
         if (r <= 0) return false;
         c += r;
         bytes -= (size_t)r;
@@ -227,6 +230,7 @@ bool recv_all(int fd, void* p, size_t bytes) {
     char* c = (char*)p;
     while (bytes > 0) {
         ssize_t r = recv(fd, c, bytes, 0);
+        if (r < 0 && errno == EINTR) continue;
         if (r <= 0) return false;
         c += r;
         bytes -= (size_t)r;
@@ -261,15 +265,21 @@ int acquire_helper(int* fd) {
     }
 }
 
+std::atomic<int64_t> g_helper_calls{0}, g_helper_failures{0}, g_inproc_calls{0};
+
 void release_helper(int i, bool ok) {
     std::lock_guard<std::mutex> lk(g_hmu);
     Helper& h = g_helpers[i];
     if (!ok) {
+        // this helper is gone: close it and let the next request start a
+        // fresh one in its place (the failed call runs in-process)
+        g_helper_failures++;
         close(h.fd);
         h.fd = -1;
         if (h.pid > 0) { kill(h.pid, SIGKILL); waitpid(h.pid, nullptr, 0); }
         h.pid = -1;
-        g_helpers_broken = true;  // fall back to in-process calls from now on
+        if (spawn_helper(h)) h.busy = false;
+        else g_helpers_broken = true;  // helpers cannot be started: in-process calls from now on
     }
     h.busy = false;
     g_hcv.notify_one();
@@ -296,11 +306,13 @@ int metis_kway(int64_t n, int64_t m, int64_t* xadj, int64_t* adj, int64_t* vw, i
                       recv_all(fd, out, sizeof(out)) && recv_all(fd, part, sizeof(int64_t) * n);
             release_helper(hi, ok);
             if (ok) {
+                g_helper_calls++;
                 *obj = out[1];
                 return (int)out[0];
             }
         }
     }
+    g_inproc_calls++;
     std::lock_guard<std::mutex> lk(g_metis_inproc);
     metis_idx_t nn = n, ncon = 1, np = nparts;
     metis_real_t u = ub;
@@ -527,6 +539,19 @@ int jet_prof_phases(int on, uint64_t* out) {
     cudaFree(g_pclk);
     g_pclk = nullptr;
     return rc;
+}
+
+int jet_metis_call_stats(int64_t* out) {
+    if (!out) return JET_ERR_INVALID;
+    out[0] = g_helper_calls.load();
+    out[1] = g_helper_failures.load();
+    out[2] = g_inproc_calls.load();
+    {
+        std::lock_guard<std::mutex> lk(g_hmu);
+        out[3] = (int64_t)g_helpers.size();
+        out[4] = g_helpers_broken ? 1 : 0;
+    }
+    return JET_OK;
 }
 
 int jet_test_inject_metis_failures(int count) { return g_metis_fail.exchange(count < 0 ? 0 : count); }
