@@ -840,16 +840,9 @@ def main():
         serving = run_serving(jet, dev, args.serving, args.workers, 120 << 30, nmax=args.serving_nmax,
                               pool=args.serving_pool, rates=[float(x) for x in args.serving_rates.split(",") if x])
     stage("serving done")
-    # the oracle's partition of a smaller power-law graph runs in a child
-    # process from here on, beside the power-law leg's GPU work (it would take
-    # host cores from the batched and served legs)
-    chk = None
-    if args.powerlaw_scale > 0 and args.check_scale > 0 and rank == 0:
-        chk = start_oracle_check(jet, dev, args.check_scale)
     powerlaw = None
     if args.powerlaw_scale > 0 and rank == 0:
-        powerlaw = run_powerlaw(jet, dev, args.powerlaw_scale, cpu_scale=(args.powerlaw_scale - 3) if cpu_cores else 0,
-                                check=chk)
+        powerlaw = run_powerlaw(jet, dev, args.powerlaw_scale, cpu_scale=(args.powerlaw_scale - 3) if cpu_cores else 0)
 
     if rank != 0:
         if ws > 1:
@@ -890,6 +883,11 @@ def main():
     if ws == 1 and not args.no_cpu_baseline:
         dt, ocut, oimb = reference_partition(host_graph(g), wl, 1)
         stage("CPU baseline done")
+    if powerlaw is not None and args.check_scale > 0:
+        # last, alone: the oracle's partition of a smaller power-law graph in
+        # a child process (its host work would disturb the other legs)
+        powerlaw["oracle_check"] = finish_oracle_check(jet, start_oracle_check(jet, dev, args.check_scale))
+        stage("oracle check done")
         cpu_base = {"value": 1.0 / dt, "unit": "graphs/s", "cores": cpu_cores, "kind": "reference",
                     "sample": "one full partition of the same graph by the reference's jet_host path on %d OpenMP "
                               "threads, cut %d" % (cpu_cores, ocut)}
