@@ -272,7 +272,9 @@ int jet_prof_enable(int on);
  * phases 0-23, then their counts.  Phases: 0 LP select, 1 afterburner,
  * 2 hub afterburner, 3 rebalance prep, 4 rebalance select, 5 bucket scan,
  * 6 candidate sort, 7 eviction, 8 strong tail, 9 apply, 10 update subtract,
- * 11 update add + mark, 12 row rebuild, 13 cut change, 14 control, 15 copy. */
+ * 11 update add + mark, 12 row rebuild, 13 cut change, 14 control, 15 copy,
+ * 16 cookie cutter, 17 strong destinations, 18 strong re-draws, 19 sorted
+ * weight prefix. */
 int jet_prof_phases(int on, uint64_t* out);
 int jet_prof_read(double* ms, double* bytes, int64_t* launches);
 
@@ -294,10 +296,11 @@ int64_t jet_launch_count(void);
  *     connectivity table of `cap` slots (k parts) with the table-build insert;
  *     JET_ERR_OVERFLOW when the probe bound flagged a full table. */
 int jet_test_inject_metis_failures(int count);
-/* Coarsest-graph Metis calls of this process: out[5] = {calls served by helper
- * processes, helper calls that failed (rerun in-process, the helper
+/* Coarsest-graph Metis calls of this process: out[6] = {calls served by helper
+ * processes, helper calls whose transfer failed (rerun in-process, the helper
  * replaced), in-process calls, helpers started, 1 if helpers could not be
- * started}. */
+ * started, helper calls on which Metis reported an error (rerun in-process
+ * once)}. */
 int jet_metis_call_stats(int64_t* out);
 int jet_test_grid_barrier(int blocks, int absent_block, int spin_cap_log2, int rounds, int* passed);
 int jet_test_table_overflow(int cap, int k, int nparts, int* claimed);

@@ -64,13 +64,14 @@ EXPORTED_SYMBOLS = [
 
 def metis_call_stats() -> dict:
     """Where this process's coarsest-graph Metis calls ran (jet_metis_call_stats)."""
-    out = (ctypes.c_int64 * 5)()
+    out = (ctypes.c_int64 * 6)()
     _check(load().jet_metis_call_stats(out))
     return dict(helper_calls=out[0], helper_failures=out[1], inprocess_calls=out[2], helpers=out[3],
-                helpers_unavailable=bool(out[4]))
+                helpers_unavailable=bool(out[4]), helper_metis_errors=out[5])
 
 PHASES = ["lp_select", "afterburn", "afterburn_hub", "reb_prep", "reb_select", "bucket_scan", "cand_sort", "evict",
-          "strong_tail", "apply", "update_sub", "update_add", "rebuild", "cut", "control", "copy"]
+          "strong_tail", "apply", "update_sub", "update_add", "rebuild", "cut", "control", "copy", "cookie",
+          "strong_first", "redraw", "weight_scan"]
 
 
 def prof_phases(on: bool):

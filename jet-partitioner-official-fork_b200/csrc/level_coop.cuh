@@ -26,30 +26,47 @@ struct GridBar {
 
 // Returns false when the loop must stop (a barrier timed out somewhere).
 // A wait gives up after spin_cap polls (2^26, about 4 s, by default).
+//
+// Thread 0 of each block arrives with a release-acquire atomic add on the
+// arrival counter: the block's earlier writes, ordered before it by
+// __syncthreads, are released with it.  The last block to arrive resets the
+// counter and publishes the next generation with a release store; the others
+// poll the generation with acquire loads, so every block's writes are
+// visible to every block after the barrier.
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 __device__ __forceinline__ bool grid_sync(GridBar* gb, int* err, long long spin_cap = (1ll << 26)) {
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned int* vgen = &gb->gen;
-        unsigned int g = *vgen;
-        __threadfence();
-        unsigned int arrived = atomicAdd(&gb->count, 1u) + 1u;
+        unsigned int g = ld_acquire_gpu(&gb->gen);
+        unsigned int arrived = atom_add_acq_rel_gpu(&gb->count, 1u) + 1u;
         if (arrived == gridDim.x) {
-            gb->count = 0;
-            __threadfence();
-            atomicAdd(&gb->gen, 1u);
+            gb->count = 0;  // ordered before the release below; nobody arrives again before it
+            st_release_gpu(&gb->gen, g + 1u);
         } else {
             long long spins = 0;
-            while (*vgen == g) {
-                if (((volatile int*)&gb->abort)[0]) break;
+            while (ld_acquire_gpu(&gb->gen) == g) {
+                if ((spins & 63) == 63 && ((volatile int*)&gb->abort)[0]) break;
                 if (++spins > spin_cap) {
                     atomicOr(err, ERRF_SPIN);
                     atomicExch(&gb->abort, 1);
                     break;
                 }
-                if (spins > 64) __nanosleep(64);
+                if (spins > 256) __nanosleep(32);
             }
         }
-        __threadfence();
     }
     __syncthreads();
     return ((volatile int*)&gb->abort)[0] == 0;
@@ -182,9 +199,11 @@ struct CoopScratch {
 
 // Rebalance tail over the grid (sort_candidates + k_evict_sorted [+ strong]).
 template <bool CL, bool STRONG, class O, class E, class W>
-__device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>& rb, CoopScratch<O, E, W>& cs, int bits) {
+__device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>& rb, CoopScratch<O, E, W>& cs, int bits,
+                                              PhaseClock& pc) {
     int* err = &a.dev->err;
     if (!grid_scan<CL, W>(GetArray<W>{rb.buckets}, (int64_t)rb.t_minibuckets + 1, rb.boff, cs.wsum, cs.bar, err)) return false;
+    pc.mark(PH_REB_SCAN);
     const int64_t n = a.g.n;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t(*cnt)[RS_BINS] = (uint32_t(*)[RS_BINS])smem_raw;  // 32 x 256 counters (dynamic shared memory)
@@ -204,9 +223,11 @@ __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>
         kin = kd;
         vin = vd;
     }
+    pc.mark(PH_REB_SORT);
     rb.skey = kin;
     rb.sval = vin;
     if (!grid_scan<CL, W>(GetSortedWeight<O, W>{kin, vin, a.g.vw, rb.none_key}, n, cs.wpre, cs.wsum, cs.bar, err)) return false;
+    pc.mark(PH_WEIGHT_SCAN);
     rb.wpre = cs.wpre;
     if (STRONG) {
         for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.k; p += gridDim.x * blockDim.x) rb.evict_adjust[p] = 0;
@@ -215,13 +236,17 @@ __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>
     if (STRONG) d_evict_sorted<true, O, E, W>(a, rb);
     else d_evict_sorted<false, O, E, W>(a, rb);
     if (!level_sync<CL>(cs.bar, err)) return false;
+    pc.mark(PH_REB_EVICT);
     if (STRONG) {
         if (blockIdx.x == 0) d_cookie<O, E, W>(a, rb);
         if (!level_sync<CL>(cs.bar, err)) return false;
+        pc.mark(PH_COOKIE);
         d_strong_first<O, E, W>(a, rb);
         if (!level_sync<CL>(cs.bar, err)) return false;
+        pc.mark(PH_STRONG_FIRST);
         if (blockIdx.x == 0) d_strong_redraw<O, E, W>(a, rb);
         if (!level_sync<CL>(cs.bar, err)) return false;
+        pc.mark(PH_REDRAW);
     }
     return true;
 }
@@ -283,9 +308,9 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             }
             if (!level_sync<CL>(cs.bar, err)) return;
             pc.mark(PH_REB_SELECT);
-            bool ok = mode == MODE_WEAK ? coop_reb_tail<CL, false, O, E, W>(a, rb, cs, bits) : coop_reb_tail<CL, true, O, E, W>(a, rb, cs, bits);
+            bool ok = mode == MODE_WEAK ? coop_reb_tail<CL, false, O, E, W>(a, rb, cs, bits, pc)
+                                        : coop_reb_tail<CL, true, O, E, W>(a, rb, cs, bits, pc);
             if (!ok) return;
-            pc.mark(PH_REB_EVICT);
         }
         // perform_moves (src/jet_refiner.hpp:905-955)
         d_apply_moves<O, E, W>(a, 0);

@@ -96,11 +96,13 @@ __device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb,
     if (STRONG) {
         d_cookie<O, E, W>(a, rb);
         __syncthreads();
+        pc.mark(PH_COOKIE);
         d_strong_first<O, E, W>(a, rb);
         __syncthreads();
+        pc.mark(PH_STRONG_FIRST);
         d_strong_redraw<O, E, W>(a, rb);
         __syncthreads();
-        pc.mark(PH_STRONG_TAIL);
+        pc.mark(PH_REDRAW);
     }
 }
 

@@ -104,7 +104,8 @@ struct RefArgs {
 static constexpr int PHASE_SLOTS = 24;
 enum PhaseId : int {
     PH_LP_SELECT = 0, PH_AFTERBURN, PH_AFTERBURN_HUB, PH_REB_PREP, PH_REB_SELECT, PH_REB_SCAN, PH_REB_SORT, PH_REB_EVICT,
-    PH_STRONG_TAIL, PH_APPLY, PH_UPDATE_SUB, PH_UPDATE_ADD, PH_REBUILD, PH_CUT, PH_CTL, PH_COPY, PH_COUNT
+    PH_STRONG_TAIL, PH_APPLY, PH_UPDATE_SUB, PH_UPDATE_ADD, PH_REBUILD, PH_CUT, PH_CTL, PH_COPY,
+    PH_COOKIE, PH_STRONG_FIRST, PH_REDRAW, PH_WEIGHT_SCAN, PH_COUNT
 };
 struct PhaseClock {
     unsigned long long* out;

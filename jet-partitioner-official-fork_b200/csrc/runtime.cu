@@ -265,7 +265,7 @@ int acquire_helper(int* fd) {
     }
 }
 
-std::atomic<int64_t> g_helper_calls{0}, g_helper_failures{0}, g_inproc_calls{0};
+std::atomic<int64_t> g_helper_calls{0}, g_helper_failures{0}, g_inproc_calls{0}, g_helper_metis_errors{0};
 
 void release_helper(int i, bool ok) {
     std::lock_guard<std::mutex> lk(g_hmu);
@@ -304,11 +304,20 @@ int metis_kway(int64_t n, int64_t m, int64_t* xadj, int64_t* adj, int64_t* vw, i
                       send_all(fd, xadj, sizeof(int64_t) * (n + 1)) && send_all(fd, adj, sizeof(int64_t) * m) &&
                       send_all(fd, vw, sizeof(int64_t) * n) && send_all(fd, ew, sizeof(int64_t) * m) &&
                       recv_all(fd, out, sizeof(out)) && recv_all(fd, part, sizeof(int64_t) * n);
-            release_helper(hi, ok);
-            if (ok) {
+            const bool metis_ok = ok && out[0] == 1;  // METIS_OK
+            // a helper whose Metis reported an error is replaced too: Metis
+            // state left from its earlier calls must not reach later ones
+            release_helper(hi, metis_ok);
+            if (metis_ok) {
                 g_helper_calls++;
                 *obj = out[1];
-                return (int)out[0];
+                return 1;
+            }
+            if (ok) {
+                // Metis failed in the helper: rerun the call once in-process
+                g_helper_calls++;
+                g_helper_metis_errors++;
+                g_helper_failures--;  // release_helper counted it as a transfer failure
             }
         }
     }
@@ -551,6 +560,7 @@ int jet_metis_call_stats(int64_t* out) {
         out[3] = (int64_t)g_helpers.size();
         out[4] = g_helpers_broken ? 1 : 0;
     }
+    out[5] = g_helper_metis_errors.load();
     return JET_OK;
 }
 
