@@ -348,15 +348,17 @@ REFINE_CLASSES = ["conn_build", "lp_select", "afterburn", "reb_select", "reb_sor
 
 def run_class_profile(jet, part_fn, cfg, g, seed, stream):
     """Profiling pass (after the timed region): one more partition of the
-    same graph with every level's refinement on the host-driven loop, so that
-    each refinement kernel class is bracketed by CUDA events on the launching
-    stream, and the library turns device-side counts of every iteration into
-    the class's algorithmic bytes.  Returns per class: device ms, bytes,
+    same graph in which the levels the timed run gives to the CUDA-graph
+    driver (those above the persistent kernels' bounds) run on the host-driven
+    loop instead, so that each refinement kernel class is bracketed by CUDA
+    events on the launching stream, and the library turns device-side counts
+    of every iteration into the class's algorithmic bytes.  The smaller levels
+    keep their persistent one-kernel loops (no classes to bracket there).  Returns per class: device ms, bytes,
     launches, achieved GB/s and fraction of the HBM peak, share of the summed
     class time; plus the pass's own wall time."""
     import torch
     peak = _hbm_peak()
-    prev = jet.set_refine_drivers(0)
+    prev = jet.set_refine_drivers(jet.DRIVER_ALL & ~jet.DRIVER_GRAPH)
     try:
         torch.cuda.synchronize()
         jet.prof_enable(True)
@@ -386,9 +388,9 @@ def run_class_profile(jet, part_fn, cfg, g, seed, stream):
             break
     byt = sum(classes[c]["bytes"] for c in cover)
     ms = sum(classes[c]["ms"] for c in cover)
-    return {"how": "one partition with every refinement level on the host-driven loop (jet_set_refine_drivers(0)); "
-                   "CUDA events around each kernel class on the launching stream; algorithmic bytes from device-side "
-                   "counts per iteration", "pass_ms": 1000 * wall, "class_ms_total": total,
+    return {"how": "one partition with the graph-driven levels on the host-driven loop (jet_set_refine_drivers(ALL & "
+                   "~GRAPH)); CUDA events around each kernel class on the launching stream; algorithmic bytes from "
+                   "device-side counts per iteration", "pass_ms": 1000 * wall, "class_ms_total": total,
             "peak_gbs": peak["value"], "peak_source": peak["source"], "dominant": ranked[0] if ranked else None,
             "classes": classes, "cover_90pct": cover,
             "cover_90pct_frac": (byt / (ms / 1000.0) / 1e9) / peak["value"] if ms > 0 else None}

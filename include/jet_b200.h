@@ -333,15 +333,19 @@ void jet_free_host(void* ptr);
  * grid kernel (n <= 131072, nnz <= 2^21, k <= 512), a CUDA graph with
  * conditional nodes, else the host loop.  JET_DRIVER_CTA_SMEM lets the
  * one-CTA loop keep the level's mutable state in shared memory (as much of
- * it as fits); without it that state stays in global memory.  Returns the
- * previous mask. */
+ * it as fits); without it that state stays in global memory.
+ * JET_DRIVER_REB_QUEUE lets rebalancing order only the candidates whose
+ * place in their bucket decides their eviction (one block, when they fit);
+ * without it every rebalance sorts all candidates.  Returns the previous
+ * mask. */
 enum {
     JET_DRIVER_CTA = 1,
     JET_DRIVER_COOP = 2,
     JET_DRIVER_GRAPH = 4,
     JET_DRIVER_CLUSTER = 8,
     JET_DRIVER_CTA_SMEM = 16,
-    JET_DRIVER_ALL = 31
+    JET_DRIVER_REB_QUEUE = 32,
+    JET_DRIVER_ALL = 63
 };
 int jet_set_refine_drivers(int mask);
 

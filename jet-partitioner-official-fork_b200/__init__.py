@@ -88,7 +88,7 @@ def prof_phases(on: bool):
     return res
 
 # level-loop drivers (jet_set_refine_drivers)
-DRIVER_CTA, DRIVER_COOP, DRIVER_GRAPH, DRIVER_CLUSTER, DRIVER_CTA_SMEM, DRIVER_ALL = 1, 2, 4, 8, 16, 31
+DRIVER_CTA, DRIVER_COOP, DRIVER_GRAPH, DRIVER_CLUSTER, DRIVER_CTA_SMEM, DRIVER_REB_QUEUE, DRIVER_ALL = 1, 2, 4, 8, 16, 32, 63
 
 
 class JetError(RuntimeError):

@@ -146,6 +146,8 @@ int64_t launch_counter();
 int refine_drivers();
 // The one-CTA level loop may keep its state in shared memory (JET_DRIVER_CTA_SMEM).
 bool cta_smem_resident();
+// Rebalancing may order only the queued candidates (JET_DRIVER_REB_QUEUE).
+bool reb_queue_enabled();
 // JET_DEBUG_TIMING set in the environment: phase timings go to stderr.
 bool debug_timing();
 // Host clock in milliseconds (steady).

@@ -195,6 +195,7 @@ struct CoopScratch {
     O* sv1;
     W* wpre;             // prefix of candidate weights in sorted order (n)
     O* marked;           // rows to rebuild after a large move set (n)
+    int qcap;            // queued candidates block 0 can order in its dynamic shared memory
 };
 
 // Rebalance tail over the grid (sort_candidates + k_evict_sorted [+ strong]).
@@ -206,6 +207,30 @@ __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>
     pc.mark(PH_REB_SCAN);
     const int64_t n = a.g.n;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (rb.queue) {
+        // the grid classifies; block 0 orders the queue (when it fits) and
+        // finishes the rebalance while the other blocks wait at the barrier
+        d_reb_classify<STRONG, O, E, W>(a, rb, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+        if (!level_sync<CL>(cs.bar, err)) return false;
+        pc.mark(PH_REB_SORT);
+        volatile RefDev<O, W>* vd = a.dev;
+        const O count = vd->nord;
+        const int fb = vd->reb_fb || count > (O)cs.qcap;
+        if (!fb && blockIdx.x == 0) d_reb_queue_tail<STRONG, O, E, W>(a, rb, count, (uint64_t*)smem_raw);
+        // every block has read the queue state before block 0 resets it
+        if (!level_sync<CL>(cs.bar, err)) return false;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            a.dev->nord_last = count;
+            a.dev->reb_fb_taken = fb;
+            a.dev->nord = 0;
+            a.dev->reb_fb = 0;
+            if (fb) a.dev->nmoves = 0;  // the full sort below decides every move again
+        }
+        if (!fb) {
+            pc.mark(PH_REB_EVICT);
+            return true;
+        }
+    }
     uint32_t(*cnt)[RS_BINS] = (uint32_t(*)[RS_BINS])smem_raw;  // 32 x 256 counters (dynamic shared memory)
     // stable sort of (bucket id, vertex) pairs
     int passes = (bits + 7) / 8;
@@ -289,8 +314,9 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             pc.mark(PH_AFTERBURN_HUB);
         } else {
             RebArgs<O, W>& rb = mode == MODE_WEAK ? rbw : rbs;
+            // bucket totals cleared while block 0 lists the parts (neither
+            // reads what the other writes)
             coop_zero<O, E, W>(rb.buckets, (int64_t)rb.t_minibuckets + 1 + rb.width);
-            if (!level_sync<CL>(cs.bar, err)) return;
             if (blockIdx.x == 0) {
                 if (mode == MODE_WEAK) d_weak_prep<O, E, W>(a, rb);
                 else d_strong_prep<O, E, W>(a, rb);

@@ -52,6 +52,30 @@ __device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb,
     const O n = a.g.n;
     block_scan_global<W>(rb.buckets, rb.boff, (int64_t)rb.t_minibuckets + 1);
     pc.mark(PH_REB_SCAN);
+    if (rb.queue) {
+        // only the candidates whose in-bucket order matters are sorted (they
+        // fit: at most n <= P of them)
+        __shared__ O s_count;
+        __shared__ int s_fb;
+        d_reb_classify<STRONG, O, E, W>(a, rb, threadIdx.x, blockDim.x);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_count = a.dev->nord;
+            s_fb = a.dev->reb_fb;
+            a.dev->nord_last = s_count;
+            a.dev->reb_fb_taken = s_fb;
+            a.dev->nord = 0;
+            a.dev->reb_fb = 0;
+            if (s_fb) a.dev->nmoves = 0;  // the full sort below decides every move again
+        }
+        __syncthreads();
+        pc.mark(PH_REB_SORT);
+        if (!s_fb) {
+            d_reb_queue_tail<STRONG, O, E, W>(a, rb, s_count, keys);
+            pc.mark(PH_REB_EVICT);
+            return;
+        }
+    }
     for (int i = threadIdx.x; i < P; i += blockDim.x) {
         uint64_t key = ~0ull;
         if (i < n) {

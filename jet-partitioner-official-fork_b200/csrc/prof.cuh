@@ -18,6 +18,7 @@ struct ProfCounts {
     unsigned long long cand, cand_deg;
     unsigned long long moves, moves_deg;
     unsigned long long marked, marked_deg, marked_cap;
+    unsigned long long reb_cand;  // rebalance candidates (vertices with a bucket)
 };
 
 // Block-wide sum of up to three values, one atomic each per block.
@@ -79,6 +80,14 @@ __global__ void __launch_bounds__(BLOCK) k_prof_marked(RefArgs<O, E, W> a, ProfC
         }
     }
     prof_block_add(m, d, cap, &c->marked, &c->marked_deg, &c->marked_cap);
+}
+
+// Rebalance candidates: vertices given a bucket by the selection.
+template <class O>
+__global__ void __launch_bounds__(BLOCK) k_prof_bid(const O* bid, int64_t n, unsigned long long* cnt) {
+    unsigned long long c = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) c += bid[i] >= 0;
+    prof_block_add(c, 0ull, 0ull, cnt, nullptr, nullptr);
 }
 
 }  // namespace jetb

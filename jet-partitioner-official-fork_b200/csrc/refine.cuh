@@ -62,6 +62,11 @@ struct RefDev {
     part_t total_undersized;
     int err;
     int large;            // this iteration used update_large
+    O nord;               // rebalance: candidates queued for in-bucket ordering
+    O nord_last;          // (their count in the last rebalance, for profiling)
+    int reb_fb;           // rebalance: the queue cannot be used (fallback to the full sort)
+    int reb_fb_taken;     // the last rebalance took the fallback
+    int reb_fb_count[2];  // fallbacks taken inside the current level graph (weak, strong)
 };
 // Copied to pinned host memory once per iteration.
 struct IterResult {
@@ -983,6 +988,8 @@ struct RebArgs {
     uint32_t none_key;     // key of non-candidates (sorted last)
     O* redraw;             // strong rebalance: vertices needing a re-drawn position
     part_t* redraw_p;      // and the chunk they stopped at
+    O* ordl;               // candidates whose in-bucket order decides their eviction
+    int queue;             // eviction from the queue allowed (else the full sort)
 };
 
 // B(x): the offset the reference reads for bucket x -- scanned for
@@ -1300,9 +1307,9 @@ __global__ void __launch_bounds__(1024) k_cookie(RefArgs<O, E, W> a, RebArgs<O, 
 // end; only those draws depend on order (they advance one shared cursor),
 // so they are queued here and replayed in vertex order by k_strong_redraw.
 template <class O, class E, class W>
-__device__ __forceinline__ void d_strong_first(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_strong_first(RefArgs<O, E, W> a, RebArgs<O, W> rb, int64_t start, int64_t stride) {
     O count = a.dev->nmoves;
-    for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < count; x += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t x = start; x < count; x += stride) {
         O v = a.moves[x];
         part_t pv = a.part[v];
         W sc = rb.score[v] + rb.boff[rb.bid[v]] - rb.evict_adjust[pv];
@@ -1332,6 +1339,10 @@ __device__ __forceinline__ void d_strong_first(RefArgs<O, E, W> a, RebArgs<O, W>
     }
 }
 template <class O, class E, class W>
+__device__ __forceinline__ void d_strong_first(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    d_strong_first<O, E, W>(a, rb, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+template <class O, class E, class W>
 __global__ void k_strong_first(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_strong_first<O, E, W>(a, rb); }
 
 // One block: sorts the queued vertices by id and replays their draws in order.
@@ -1352,11 +1363,21 @@ __device__ __forceinline__ void block_sort_keys(K* key, int P) {
         }
     }
 }
+// The replay is one thread's serial walk (each draw advances the shared
+// cursor), so what it reads is staged first: the chunk bounds in shared
+// memory (when k fits), and each vertex's weight, chunk and part are loaded
+// one vertex ahead of their use.
+static constexpr int REDRAW_ES_CAP = 513;
 template <class O, class E, class W>
 __device__ __forceinline__ void d_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
     __shared__ O list[REDRAW_CAP];
+    __shared__ W es_s[REDRAW_ES_CAP];
     O cnt = a.dev->nredraw;
     if (cnt == 0) return;
+    const bool stage = a.k + 1 <= REDRAW_ES_CAP;
+    if (stage)
+        for (int p = threadIdx.x; p <= a.k; p += blockDim.x) es_s[p] = rb.evict_start[p];
+    const W* es = stage ? es_s : rb.evict_start;
     bool fits = cnt <= REDRAW_CAP;
     if (fits) {
         int P = 1;
@@ -1364,31 +1385,241 @@ __device__ __forceinline__ void d_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W
         for (int i = threadIdx.x; i < P; i += blockDim.x) list[i] = i < (int)cnt ? rb.redraw[i] : std::numeric_limits<O>::max();
         __syncthreads();
         block_sort_keys<O>(list, P);
-    } else if (threadIdx.x == 0) {
-        atomicOr(&a.dev->err, 16);  // more draws than the replay buffer: order falls back to queue order
+    } else {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicOr(&a.dev->err, 16);  // more draws than the replay buffer: order falls back to queue order
     }
     if (threadIdx.x != 0) return;
     W cursor = a.dev->vw_cursor;
+    O v = fits ? list[0] : rb.redraw[0];
+    W w = a.g.vw[v];
+    int p = rb.redraw_p[v];
+    part_t pv = a.part[v];
     for (O x = 0; x < cnt; x++) {
-        O v = fits ? list[x] : rb.redraw[x];
-        W w = a.g.vw[v];
-        int p = rb.redraw_p[v];
-        part_t dest = a.part[v];
+        O vn = v;
+        W wn = w;
+        int pn = p;
+        part_t pvn = pv;
+        if (x + 1 < cnt) {
+            vn = fits ? list[x + 1] : rb.redraw[x + 1];
+            wn = a.g.vw[vn];
+            pn = rb.redraw_p[vn];
+            pvn = a.part[vn];
+        }
+        part_t dest = pv;
         int guard = 0;
         while (p < a.k) {
             W sc = cursor;
             cursor += w;
-            while (p <= a.k && rb.evict_start[p] <= sc) p++;
+            while (p <= a.k && es[p] <= sc) p++;
             p--;
-            if (p < a.k && w / 2 <= rb.evict_start[p + 1] - sc) { dest = p; break; }
+            if (p < a.k && w / 2 <= es[p + 1] - sc) { dest = p; break; }
             if (++guard > 4 * a.k + 64) { atomicOr(&a.dev->err, ERRF_SPIN); break; }
         }
         a.dest[v] = dest;
+        v = vn;
+        w = wn;
+        p = pn;
+        pv = pvn;
     }
     a.dev->vw_cursor = cursor;
 }
 template <class O, class E, class W>
 __global__ void __launch_bounds__(1024) k_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W> rb) { d_strong_redraw<O, E, W>(a, rb); }
+
+// ---------------------------------------------------------------- eviction from a short queue
+// A candidate's eviction score (get_evictions, src/jet_refiner.hpp:392-409)
+// is the offset of its bucket inside its part's bucket range plus "within",
+// the weight of the bucket's candidates before it in vertex order; it leaves
+// while the score is below its part's excess.  Weights are non-negative, so
+// within lies in [0, bucket total - own weight]: a bucket whose offset
+// reaches the excess keeps every candidate, and (weak) a bucket that ends
+// below the excess loses every one, whatever their order.  Only the
+// candidates of the buckets in between -- weak: the bucket that straddles the
+// excess, one per part; strong: also every bucket that leaves, since the
+// destination draw reads each evicted vertex's score -- need their place in
+// the bucket.  d_reb_classify decides the rest and queues those on rb.ordl;
+// d_reb_ordered orders the queue in one block.  The moves, scores and
+// adjustments are those of the full sort (sort_candidates + d_evict_sorted),
+// which stays as the fallback for what this cannot take: a weak bucket id
+// past its part's range (gain bucket 50 shares the next part's first bucket,
+// so one bucket would hold two parts' candidates), a negative vertex weight,
+// or a queue longer than the block holds.
+template <bool STRONG, class O, class E, class W>
+__device__ __forceinline__ void d_reb_classify(RefArgs<O, E, W> a, RebArgs<O, W> rb, int64_t start, int64_t stride) {
+    const int64_t n = a.g.n;
+    const int64_t rounds = ceil_div<int64_t>(n, stride);
+    for (int64_t r = 0; r < rounds; r++) {  // the same count in every lane: warp_append needs the whole warp
+        const int64_t q = start + r * stride;
+        bool take = false, order = false;
+        O b = -1;
+        if (q < n) b = rb.bid[q];
+        if (b >= 0) {
+            const O i = (O)q;
+            const part_t p = a.part[i];
+            const O begin = (O)p * rb.width;
+            const W w = a.g.vw[i];
+            if ((!STRONG && b >= begin + rb.width) || w < 0) {
+                atomicOr(&a.dev->reb_fb, 1);
+            } else {
+                const W base = rb.boff[b] - rb.boff[begin];
+                const W limit = a.sizes[p] - rb.size_max;
+                if (base < limit) {
+                    if (!STRONG && base + rb.buckets[b] < limit) take = true;
+                    else order = true;
+                }
+            }
+        }
+        O s = warp_append(&a.dev->nmoves, take);
+        if (take) a.moves[s] = (O)q;
+        O t = warp_append(&a.dev->nord, order);
+        if (order) rb.ordl[t] = (O)q;
+    }
+}
+
+// Inclusive sum of v over runs that begin where head is set, across the
+// block (every thread calls it, one value each).  carry is the sum of the
+// run left open by the previous call and is updated for the next call.
+template <class T>
+__device__ __forceinline__ T block_seg_scan(T v, bool head, T& carry) {
+    __shared__ T sv[32];
+    __shared__ int sf[32];
+    __shared__ T s_last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    T x = v;
+    int f = head ? 1 : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, x, o);
+        int g = __shfl_up_sync(0xffffffffu, f, o);
+        if (lane >= o) {
+            if (!f) x += y;
+            f |= g;
+        }
+    }
+    if (lane == 31) { sv[wid] = x; sf[wid] = f; }
+    __syncthreads();
+    if (wid == 0) {
+        T y = lane < nw ? sv[lane] : T(0);
+        int g = lane < nw ? sf[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            T y2 = __shfl_up_sync(0xffffffffu, y, o);
+            int g2 = __shfl_up_sync(0xffffffffu, g, o);
+            if (lane >= o) {
+                if (!g) y += y2;
+                g |= g2;
+            }
+        }
+        if (lane < nw) { sv[lane] = y; sf[lane] = g; }
+    }
+    __syncthreads();
+    if (!f && wid > 0) { x += sv[wid - 1]; f = sf[wid - 1]; }
+    if (!f) x += carry;
+    if (threadIdx.x == blockDim.x - 1) s_last = x;
+    __syncthreads();
+    carry = s_last;
+    return x;
+}
+
+// One block: the queued candidates sorted by (bucket, vertex) in shared
+// memory (keys: at least count entries rounded up to a power of two), the
+// weight prefix inside each bucket, and the eviction test of
+// d_evict_sorted for them (strong: with the scores and part adjustments).
+template <bool STRONG, class O, class E, class W>
+__device__ __forceinline__ void d_reb_ordered(RefArgs<O, E, W> a, RebArgs<O, W> rb, O count, uint64_t* keys) {
+    int P = 1;
+    while (P < (int)count) P <<= 1;
+    for (int q = threadIdx.x; q < P; q += blockDim.x) {
+        uint64_t key = ~0ull;
+        if (q < (int)count) {
+            const O i = rb.ordl[q];
+            key = ((uint64_t)(uint32_t)rb.bid[i] << 32) | (uint32_t)i;
+        }
+        keys[q] = key;
+    }
+    if (STRONG)
+        for (int p = threadIdx.x; p < a.k; p += blockDim.x) rb.evict_adjust[p] = 0;
+    __syncthreads();
+    block_sort_keys<uint64_t>(keys, P);
+    W carry = 0;
+    for (int base = 0; base < (int)count; base += blockDim.x) {
+        const int q = base + threadIdx.x;
+        const bool in = q < (int)count;
+        const uint64_t key = in ? keys[q] : 0ull;
+        const uint32_t b32 = (uint32_t)(key >> 32);
+        const bool head = in && (q == 0 || (uint32_t)(keys[q - 1] >> 32) != b32);
+        const O i = (O)(uint32_t)key;
+        const W w = in ? a.g.vw[i] : W(0);
+        const W incl = block_seg_scan<W>(w, head, carry);
+        bool take = false;
+        if (in) {
+            const O b = (O)b32;
+            const part_t p = a.part[i];
+            const O begin = (O)p * rb.width;
+            const W within = incl - w;
+            if (STRONG) rb.score[i] = within;
+            const W score = within + rb.boff[b] - rb.boff[begin];
+            const W limit = a.sizes[p] - rb.size_max;
+            if (score < limit) {
+                take = true;
+                if (STRONG && score + w >= limit) rb.evict_adjust[p] = score + w;
+            }
+        }
+        O s = warp_append(&a.dev->nmoves, take);
+        if (take) a.moves[s] = i;
+    }
+    __syncthreads();
+}
+
+// The ordered eviction and, for strong rebalancing, the cookie cutter and the
+// destination draws, all in one block.
+template <bool STRONG, class O, class E, class W>
+__device__ __forceinline__ void d_reb_queue_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb, O count, uint64_t* keys) {
+    d_reb_ordered<STRONG, O, E, W>(a, rb, count, keys);
+    if (STRONG) {
+        d_cookie<O, E, W>(a, rb);
+        __syncthreads();
+        d_strong_first<O, E, W>(a, rb, threadIdx.x, blockDim.x);
+        __syncthreads();
+        d_strong_redraw<O, E, W>(a, rb);
+        __syncthreads();
+    }
+}
+
+template <bool STRONG, class O, class E, class W>
+__global__ void __launch_bounds__(BLOCK) k_reb_classify(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+    d_reb_classify<STRONG, O, E, W>(a, rb, blockIdx.x * (int64_t)blockDim.x + threadIdx.x, (int64_t)gridDim.x * blockDim.x);
+}
+
+// One block of 1024 threads after k_reb_classify.  When the queue fits `cap`
+// keys of dynamic shared memory and nothing asked for the fallback, it
+// finishes the rebalance; otherwise it drops the moves the classification
+// queued and raises reb_fb_taken (and, inside a graph, the conditional
+// handle of the fallback's IF node).  Either way it resets the queue.
+template <bool STRONG, class O, class E, class W>
+__global__ void __launch_bounds__(1024) k_reb_ordered(RefArgs<O, E, W> a, RebArgs<O, W> rb, int cap, cudaGraphConditionalHandle h,
+                                                      int in_graph) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ O s_count;
+    __shared__ int s_fb;
+    if (threadIdx.x == 0) {
+        const O count = a.dev->nord;
+        const int fb = a.dev->reb_fb || count > (O)cap;
+        s_count = count;
+        s_fb = fb;
+        a.dev->nord_last = count;
+        a.dev->reb_fb_taken = fb;
+        a.dev->nord = 0;
+        a.dev->reb_fb = 0;
+        if (fb) a.dev->nmoves = 0;
+        if (in_graph) {
+            cudaGraphSetConditional(h, fb ? 1u : 0u);
+            a.dev->reb_fb_count[STRONG ? 1 : 0] += fb;
+        }
+    }
+    __syncthreads();
+    if (s_fb) return;
+    d_reb_queue_tail<STRONG, O, E, W>(a, rb, s_count, (uint64_t*)smem_raw);
+}
 
 // ---------------------------------------------------------------- moves
 // perform_moves part 1 (src/jet_refiner.hpp:910-931): cut change from the old

@@ -154,6 +154,7 @@ static std::atomic<int> g_drivers{JET_DRIVER_ALL};
 static thread_local int t_driver_mask = JET_DRIVER_ALL;
 int refine_drivers() { return g_drivers.load() & t_driver_mask; }
 bool cta_smem_resident() { return (g_drivers.load() & JET_DRIVER_CTA_SMEM) != 0; }
+bool reb_queue_enabled() { return (g_drivers.load() & JET_DRIVER_REB_QUEUE) != 0; }
 double host_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }

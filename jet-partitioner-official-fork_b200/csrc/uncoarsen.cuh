@@ -21,7 +21,7 @@ struct Refiner {
     DBuf<part_t> csize, dest_cache, part_work, dest, undersized;
     DBuf<uint8_t> lock, mark;
     DBuf<W> save_gain, pregain, score, sizes_curr, sizes_best, evict_adjust, evict_start, buckets;
-    DBuf<O> cand, cand_hub, moves, moves_hub, bid, sv0, sv1, redraw;
+    DBuf<O> cand, cand_hub, moves, moves_hub, bid, sv0, sv1, redraw, ordl;
     DBuf<uint32_t> sk0, sk1;
     DBuf<W> boff, wpre;
     DBuf<part_t> redraw_p;
@@ -80,7 +80,7 @@ struct Refiner {
         buckets.alloc(bucket_cap, s);
         boff.alloc(bucket_cap, s);
         sk0.alloc(n1, s); sk1.alloc(n1, s); sv0.alloc(n1, s); sv1.alloc(n1, s); wpre.alloc(n1, s);
-        redraw.alloc(n1, s); redraw_p.alloc(n1, s);
+        redraw.alloc(n1, s); redraw_p.alloc(n1, s); ordl.alloc(n1, s);
         lorder.alloc(n1, s);
         s16.alloc(n1, s);
         s32.alloc(n1, s);
@@ -150,6 +150,10 @@ struct Refiner {
         JET_CUDA(cudaFuncSetAttribute(k_conn_warp<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)warp_smem_max()));
         JET_CUDA(cudaFuncSetAttribute(k_conn_cta<O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       device_info().max_smem_optin - 1024));
+        JET_CUDA(cudaFuncSetAttribute(k_reb_ordered<false, O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(QUEUE_KEYS * sizeof(uint64_t))));
+        JET_CUDA(cudaFuncSetAttribute(k_reb_ordered<true, O, E, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)(QUEUE_KEYS * sizeof(uint64_t))));
         attrs_done = true;
     }
     static size_t warp_smem_max() { return (size_t)(BLOCK / 32) * WARP_TABLE * (sizeof(part_t) + sizeof(W)) + 16; }
@@ -281,7 +285,7 @@ struct Refiner {
     int ph[PK_COUNT];
     int ph_mark = -1;
     DBuf<ProfCounts> pcount;
-    void ph_reset() { for (int i = 0; i < PK_COUNT; i++) ph[i] = -1; ph_mark = -1; }
+    void ph_reset() { for (int i = 0; i < PK_COUNT; i++) ph[i] = -1; ph_mark = -1; phq[0] = phq[1] = -1; }
 
     void lp(const Level<O, E, W>& L) {
         auto a = args(L);
@@ -331,6 +335,9 @@ struct Refiner {
         rb.redraw = redraw.p; rb.redraw_p = redraw_p.p;
         rb.skey = nullptr; rb.sval = nullptr; rb.wpre = wpre.p;
         rb.none_key = (uint32_t)((int64_t)tmb + rb.width + 1);
+        rb.ordl = ordl.p;
+        // queue keys pack (bucket id, vertex) into 32 bits each
+        rb.queue = reb_queue_enabled() && (int64_t)L.n <= (int64_t)UINT32_MAX && bucket_cap <= (int64_t)UINT32_MAX;
         if ((int64_t)tmb + 1 + rb.width > bucket_cap) throw JetError{JET_ERR_INVALID, "bucket array too small"};
         if (clear) JET_CUDA(cudaMemsetAsync(buckets.p, 0, sizeof(W) * ((size_t)tmb + 1 + rb.width), s));
         return rb;
@@ -349,10 +356,10 @@ struct Refiner {
                                                  nullptr, e.scan, s);
     }
 
-    // rebalance_weak, src/jet_refiner.hpp:551-645.
-    void weak(const Level<O, E, W>& L, W opt, W size_max) {
+    // rebalance_weak, src/jet_refiner.hpp:551-645: destinations and bucket
+    // scores, then the eviction (the queue path, else the full sort).
+    void weak_select(const Level<O, E, W>& L, RebArgs<O, W>& rb) {
         auto a = args(L);
-        auto rb = reb_args(L, weak_max_dest(size_max), opt, size_max);
         int h = ph[PK_REB_SELECT] = prof_begin(s);
         k_weak_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
         k_weak_select_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
@@ -360,13 +367,21 @@ struct Refiner {
         if (L.n_hub > 0) { k_weak_select_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub); count_launch(); }
         JET_LAUNCH_CHECK();
         prof_end(h, PK_REB_SELECT, 0, s);
-        h = ph[PK_REB_SORT] = prof_begin(s);
+    }
+    void weak_full(const Level<O, E, W>& L, RebArgs<O, W>& rb) {
+        auto a = args(L);
+        int h = ph[PK_REB_SORT] = prof_begin(s);
         sort_candidates(L, rb);
         prof_end(h, PK_REB_SORT, reb_sort_bytes(L, rb), s);
         h = ph[PK_REB_EVICT] = prof_begin(s);
         k_evict_sorted<false, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
         JET_LAUNCH_CHECK();
         prof_end(h, PK_REB_EVICT, 0, s);
+    }
+    void weak(const Level<O, E, W>& L, W opt, W size_max) {
+        auto rb = reb_args(L, weak_max_dest(size_max), opt, size_max);
+        weak_select(L, rb);
+        if (!rb.queue || !reb_queue<false>(L, rb)) weak_full(L, rb);
     }
 
     // Algorithmic bytes of sort_candidates: the bucket scan, each radix pass
@@ -379,9 +394,8 @@ struct Refiner {
     }
 
     // rebalance_strong, src/jet_refiner.hpp:417-546.
-    void strong(const Level<O, E, W>& L, W opt, W size_max) {
+    void strong_select(const Level<O, E, W>& L, RebArgs<O, W>& rb) {
         auto a = args(L);
-        auto rb = reb_args(L, strong_max_dest(opt, size_max), opt, size_max);
         int h = ph[PK_REB_SELECT] = prof_begin(s);
         k_strong_prep<O, E, W><<<1, 1024, 0, s>>>(a, rb); count_launch();
         k_strong_score_thread<O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
@@ -389,7 +403,10 @@ struct Refiner {
         if (L.n_hub > 0) { k_strong_score_warp<O, E, W><<<grid_persistent((int64_t)L.n_hub * 32, 16), BLOCK, 0, s>>>(a, rb, L.hub_list.p, L.n_hub); count_launch(); }
         JET_LAUNCH_CHECK();
         prof_end(h, PK_REB_SELECT, 0, s);
-        h = ph[PK_REB_SORT] = prof_begin(s);
+    }
+    void strong_full(const Level<O, E, W>& L, RebArgs<O, W>& rb) {
+        auto a = args(L);
+        int h = ph[PK_REB_SORT] = prof_begin(s);
         sort_candidates(L, rb);
         prof_end(h, PK_REB_SORT, reb_sort_bytes(L, rb), s);
         h = ph[PK_REB_EVICT] = prof_begin(s);
@@ -401,6 +418,47 @@ struct Refiner {
         JET_LAUNCH_CHECK();
         prof_end(h, PK_REB_EVICT, 0, s);
     }
+    void strong(const Level<O, E, W>& L, W opt, W size_max) {
+        auto rb = reb_args(L, strong_max_dest(opt, size_max), opt, size_max);
+        strong_select(L, rb);
+        if (!rb.queue || !reb_queue<true>(L, rb)) strong_full(L, rb);
+    }
+
+    // The queue path of the eviction (d_reb_classify, k_reb_ordered): bucket
+    // offsets, the classification over every vertex, then one block orders
+    // the queue and finishes.  In a graph (h given) the ordering kernel sets
+    // h for the fallback's IF node; on the host loop this reads back whether
+    // the fallback must run, and returns false if so.
+    static constexpr int QUEUE_KEYS = 8192;  // 64 KiB of keys in k_reb_ordered's shared memory
+    int phq[2] = {-1, -1};                  // profiling brackets of the queue path
+    template <bool STRONG>
+    bool reb_queue(const Level<O, E, W>& L, RebArgs<O, W>& rb, cudaGraphConditionalHandle h = 0, bool in_graph = false) {
+        auto a = args(L);
+        set_attrs();
+        if (prof_active()) {
+            k_prof_bid<O><<<grid_persistent(L.n, 4), BLOCK, 0, s>>>(rb.bid, (int64_t)L.n, &pcount.p->reb_cand); count_launch();
+            JET_LAUNCH_CHECK();
+        }
+        phq[0] = prof_begin(s);
+        exclusive_scan_array<W>(buckets.p, (int64_t)rb.t_minibuckets + 1, boff.p, nullptr, e.scan, s);
+        k_reb_classify<STRONG, O, E, W><<<grid_persistent(L.n, 16), BLOCK, 0, s>>>(a, rb); count_launch();
+        JET_LAUNCH_CHECK();
+        prof_end(phq[0], PK_REB_SORT, 0, s);
+        phq[1] = prof_begin(s);
+        k_reb_ordered<STRONG, O, E, W><<<1, 1024, QUEUE_KEYS * sizeof(uint64_t), s>>>(a, rb, QUEUE_KEYS, h, in_graph ? 1 : 0);
+        count_launch();
+        JET_LAUNCH_CHECK();
+        prof_end(phq[1], PK_REB_EVICT, 0, s);
+        if (in_graph) return true;
+        JET_CUDA(cudaMemcpyAsync(e.hscal, dev.p, sizeof(RefDev<O, W>), cudaMemcpyDeviceToHost, s));
+        e.sync();
+        const RefDev<O, W>* d = (const RefDev<O, W>*)e.hscal;
+        q_last = (int64_t)d->nord_last;
+        q_fb_last = d->reb_fb_taken;
+        return !d->reb_fb_taken;
+    }
+    int64_t q_last = 0;
+    int q_fb_last = 0;
 
     // perform_moves, src/jet_refiner.hpp:905-955, in four parts: the moves
     // themselves (apply_moves_kernel, which also decides update_small versus
@@ -504,8 +562,28 @@ struct Refiner {
             // weak select / strong scores: every vertex's part, weight, table
             // offset and size and its whole table; bucket id and score out
             prof_add_bytes(ph[PK_REB_SELECT], n * (4 + sw + se + 4 + 4 + sw) + (double)c.csize_all * sl);
-            // eviction filter over the sorted candidates; the moves appended
-            prof_add_bytes(ph[PK_REB_EVICT], n * (4 + so + sw + 4) + T * (so + 4));
+            const double evict_full = n * (4 + so + sw + 4) + T * (so + 4);
+            if (phq[0] >= 0) {
+                O sections, tmb;
+                sections_for(L.n, sections, tmb);
+                const double nb = (double)tmb + 1, m = (double)q_last, cand = (double)c.reb_cand;
+                // queue path: bucket scan (read, write), every vertex's bucket
+                // id, each candidate's part and weight, the bucket offsets and
+                // totals and the part sizes once, the queued and the directly
+                // evicted vertices appended
+                prof_add_bytes(phq[0], 2 * nb * sw + n * so + cand * (4 + sw) + 2 * nb * sw + k * sw + (T + m) * so);
+                // ordering block: each queued vertex's id, bucket, weight and
+                // part and its two bucket offsets, the moves appended (strong:
+                // the score writes, the cookie cutter over the parts and each
+                // move's destination draw)
+                double ob = m * (so + so + sw + 4 + 2 * sw) + T * so;
+                if (kind == 2) ob += m * sw + 4.0 * k * sw + T * (so + 4 + 3 * sw + 4);
+                prof_add_bytes(phq[1], q_fb_last ? 0.0 : ob);
+                if (q_fb_last) prof_add_bytes(ph[PK_REB_EVICT], evict_full);
+            } else {
+                // eviction filter over the sorted candidates; the moves appended
+                prof_add_bytes(ph[PK_REB_EVICT], evict_full);
+            }
         }
         // apply: per move its vertex, part, destination and weight, the part
         // and destination writes, the two size updates
@@ -742,8 +820,13 @@ struct Refiner {
         size_t nw = CTA_THREADS / 32;
         size_t conn = ((nw * kw * sizeof(part_t) + 15) & ~(size_t)15) + nw * kw * sizeof(W);
         size_t rs = (size_t)32 * RS_BINS * sizeof(uint32_t);
-        return (conn > rs ? conn : rs) + 64;
+        size_t q = (size_t)COOP_QUEUE_KEYS * sizeof(uint64_t);
+        size_t b = conn > rs ? conn : rs;
+        return (b > q ? b : q) + 64;
     }
+    // rebalance candidates block 0 of the persistent grid orders in shared memory
+    static constexpr int COOP_QUEUE_KEYS = 8192;
+    int coop_qcap() const { return (int)((coop_smem() - 64) / sizeof(uint64_t)); }
     size_t coop_static_smem() const {
         static size_t bytes = [] {
             cudaFuncAttributes fa;
@@ -824,7 +907,7 @@ struct Refiner {
         LevelLists<O> li{L.warp_list.p, L.n_warp, L.hub_list.p, L.n_hub, L.group};
         RebArgs<O, W> rbw = reb_args(L, weak_max_dest(pb.size_max), pb.opt, pb.size_max, false);
         RebArgs<O, W> rbs = reb_args(L, strong_max_dest(pb.opt, pb.size_max), pb.opt, pb.size_max, false);
-        CoopScratch<O, E, W> cs{cbar.p, cwsum.p, chist.p, sk0.p, sk1.p, sv0.p, sv1.p, wpre.p, cmarked.p};
+        CoopScratch<O, E, W> cs{cbar.p, cwsum.p, chist.p, sk0.p, sk1.p, sv0.p, sv1.p, wpre.p, cmarked.p, coop_qcap()};
         int bits = bits_for((uint64_t)rbw.none_key);
         int max_iters = 1 << 22;
         RefArgs<O, E, W> a = args(L);
@@ -922,17 +1005,44 @@ struct Refiner {
             JET_CUDA(cudaGraphConditionalHandleCreate(&h.weak, G, 0, cudaGraphCondAssignDefault));
             JET_CUDA(cudaGraphConditionalHandleCreate(&h.strong, G, 0, cudaGraphCondAssignDefault));
             JET_CUDA(cudaGraphConditionalHandleCreate(&h.copy, G, 0, cudaGraphCondAssignDefault));
-            int64_t kb = 0, klp = 0, kw = 0, ks = 0, km = 0;
+            // the rebalance bodies end in an IF node holding the full sort,
+            // which k_reb_ordered opens when the queue cannot be used
+            // (a handle must belong to a node: made only where the IF exists)
+            RebArgs<O, W> rbw = reb_args(L, weak_max_dest(pb.size_max), pb.opt, pb.size_max, false);
+            RebArgs<O, W> rbs = reb_args(L, strong_max_dest(pb.opt, pb.size_max), pb.opt, pb.size_max, false);
+            cudaGraphConditionalHandle fbw = 0, fbs = 0;
+            if (rbw.queue) JET_CUDA(cudaGraphConditionalHandleCreate(&fbw, G, 0, cudaGraphCondAssignDefault));
+            if (rbs.queue) JET_CUDA(cudaGraphConditionalHandleCreate(&fbs, G, 0, cudaGraphCondAssignDefault));
+            JET_CUDA(cudaMemsetAsync(dev.p->reb_fb_count, 0, 2 * sizeof(int), s));
+            int64_t kb = 0, klp = 0, kw = 0, ks = 0, km = 0, kfw = 0, kfs = 0;
             Ctl<W>* cp = ctl.p;
             auto t0 = capture_into(G, {}, [&] { k_ctl_begin<W><<<1, 1, 0, s>>>(cp, h); count_launch(); JET_LAUNCH_CHECK(); }, &kb);
-            cudaGraph_t body, b_lp, b_weak, b_strong, b_copy;
+            cudaGraph_t body, b_lp, b_weak, b_strong, b_copy, b_fbw, b_fbs;
             add_conditional(G, t0, h.loop, cudaGraphCondTypeWhile, &body);
             cudaGraphNode_t n_lp = add_conditional(body, {}, h.lp, cudaGraphCondTypeIf, &b_lp);
             capture_into(b_lp, {}, [&] { lp(L); }, &klp);
             cudaGraphNode_t n_weak = add_conditional(body, {n_lp}, h.weak, cudaGraphCondTypeIf, &b_weak);
-            capture_into(b_weak, {}, [&] { weak(L, pb.opt, pb.size_max); }, &kw);
+            auto tw = capture_into(b_weak, {}, [&] {
+                rbw = reb_args(L, weak_max_dest(pb.size_max), pb.opt, pb.size_max);
+                weak_select(L, rbw);
+                if (rbw.queue) reb_queue<false>(L, rbw, fbw, true);
+                else weak_full(L, rbw);
+            }, &kw);
+            if (rbw.queue) {
+                add_conditional(b_weak, tw, fbw, cudaGraphCondTypeIf, &b_fbw);
+                capture_into(b_fbw, {}, [&] { weak_full(L, rbw); }, &kfw);
+            }
             cudaGraphNode_t n_strong = add_conditional(body, {n_weak}, h.strong, cudaGraphCondTypeIf, &b_strong);
-            capture_into(b_strong, {}, [&] { strong(L, pb.opt, pb.size_max); }, &ks);
+            auto ts = capture_into(b_strong, {}, [&] {
+                rbs = reb_args(L, strong_max_dest(pb.opt, pb.size_max), pb.opt, pb.size_max);
+                strong_select(L, rbs);
+                if (rbs.queue) reb_queue<true>(L, rbs, fbs, true);
+                else strong_full(L, rbs);
+            }, &ks);
+            if (rbs.queue) {
+                add_conditional(b_strong, ts, fbs, cudaGraphCondTypeIf, &b_fbs);
+                capture_into(b_fbs, {}, [&] { strong_full(L, rbs); }, &kfs);
+            }
             // (the update_small / update_large kernels all run and test the
             // device-side decision: conditional nodes around them cost more
             // than the kernels that return at once)
@@ -955,10 +1065,13 @@ struct Refiner {
             JET_CUDA(cudaGraphLaunch(X, s));
             JET_CUDA(cudaMemcpyAsync(hctl, ctl.p, sizeof(Ctl<W>), cudaMemcpyDeviceToHost, s));
             JET_CUDA(cudaMemcpyAsync(e.hres, &dev.p->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+            JET_CUDA(cudaMemcpyAsync(e.hscal, dev.p->reb_fb_count, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
             e.sync();
-            // kernels the graph ran: captured once, executed once per iteration of their kind
-            add_launches(kb + klp * c.lab_counter + kw * c.weak_iters + ks * c.strong_iters + km * c.iter_count -
-                         (kb + klp + kw + ks + km));
+            // kernels the graph ran: captured once, executed once per iteration
+            // of their kind, the full sorts once per fallback
+            const int* nfb = (const int*)e.hscal;
+            add_launches(kb + klp * c.lab_counter + kw * c.weak_iters + ks * c.strong_iters + km * c.iter_count +
+                         kfw * nfb[0] + kfs * nfb[1] - (kb + klp + kw + ks + km + kfw + kfs));
         } catch (...) {
             if (X) cudaGraphExecDestroy(X);
             cudaGraphDestroy(G);

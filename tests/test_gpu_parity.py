@@ -176,38 +176,71 @@ def test_lp_iterations_bit_exact(jet, graphs, orc, tier, kind, k):
         assert gm == wm
 
 
+@pytest.mark.parametrize("queue", [True, False], ids=["queue", "fullsort"])
 @pytest.mark.parametrize("tier", TIERS)
 @pytest.mark.parametrize("kind,k", [("grid2d", 8), ("grid3d", 16), ("rgg", 32), ("rmat", 16), ("star", 4), ("dense", 64)])
-def test_rebalance_iterations_bit_exact(jet, graphs, orc, tier, kind, k):
+def test_rebalance_iterations_bit_exact(jet, graphs, orc, tier, kind, k, queue):
     """Weak and strong rebalancing reproduce the oracle's in-order bucket
     scores and destination draws: parts, sizes, cut and tables match after
     every iteration of runs that start badly unbalanced (30% and 90% of the
     vertices piled into part 0; from the latter two weak iterations do not
-    restore balance, so strong rebalancing runs)."""
+    restore balance, so strong rebalancing runs).  Both eviction forms: the
+    queue of the candidates whose in-bucket order matters, and the sort of
+    every candidate."""
     g = make(graphs, kind, tier)
     og = orc.G.from_csr(g)
     imb = 1.10 if kind == "rmat" else 1.03
     seen = set()
-    for skew in (0.3, 0.9):
-        rng = np.random.default_rng(1)
-        part = orc.metis(og, k)
-        part[rng.random(g.n) < skew] = 0
-        for iters in (1, 2, 3, 6, 10):
-            want = orc.refine_iters(og, part, k, imb, 0.75, iters)
-            got = jet.refine_iters(g.to("cuda"), torch.from_numpy(part).cuda(), k, imb, 0.75, iters)
-            assert got["kinds"] == list(want["kinds"])
-            assert got["moves"] == list(want["moves"])
-            assert np.array_equal(host(got["part"]), want["part"])
-            assert np.array_equal(host(got["sizes"]), want["sizes"])
-            assert got["cut"] == want["cut"]
-            gm = table_multisets(host(got["off"]), host(got["ent"]), host(got["val"]), host(got["size"]))
-            assert gm == table_multisets(want["off"], want["ent"], want["val"], want["size"])
-        seen.update(want["kinds"])
-        # the cut bookkeeping matches a fresh recomputation
-        assert got["cut"] // 2 == orc.pstat(og, host(got["part"]), k)[0]
+    prev = jet.set_refine_drivers(jet.DRIVER_ALL if queue else jet.DRIVER_ALL & ~jet.DRIVER_REB_QUEUE)
+    try:
+        for skew in (0.3, 0.9):
+            seen.update(_skewed_runs(jet, orc, g, og, k, imb, skew))
+    finally:
+        jet.set_refine_drivers(prev)
     assert 1 in seen
     if kind not in ("grid2d", "star"):
         assert 2 in seen
+
+
+def _skewed_runs(jet, orc, g, og, k, imb, skew, iters_list=(1, 2, 3, 6, 10)):
+    """refine_iters from a Metis partition with a share `skew` of the
+    vertices moved to part 0, against the oracle after each count of
+    iterations; returns the iteration kinds seen."""
+    seen = set()
+    rng = np.random.default_rng(1)
+    part = orc.metis(og, k)
+    part[rng.random(g.n) < skew] = 0
+    for iters in iters_list:
+        want = orc.refine_iters(og, part, k, imb, 0.75, iters)
+        got = jet.refine_iters(g.to("cuda"), torch.from_numpy(part).cuda(), k, imb, 0.75, iters)
+        assert got["kinds"] == list(want["kinds"])
+        assert got["moves"] == list(want["moves"])
+        assert np.array_equal(host(got["part"]), want["part"])
+        assert np.array_equal(host(got["sizes"]), want["sizes"])
+        assert got["cut"] == want["cut"]
+        gm = table_multisets(host(got["off"]), host(got["ent"]), host(got["val"]), host(got["size"]))
+        assert gm == table_multisets(want["off"], want["ent"], want["val"], want["size"])
+    seen.update(want["kinds"])
+    # the cut bookkeeping matches a fresh recomputation
+    assert got["cut"] // 2 == orc.pstat(og, host(got["part"]), k)[0]
+    return seen
+
+
+@pytest.mark.parametrize("tier", ["i32", "big"])
+def test_rebalance_queue_overflow_falls_back(jet, graphs, orc, tier):
+    """A 250 x 250 mesh with 90% of its vertices piled into one part: the
+    evictions' in-bucket order matters for tens of thousands of candidates,
+    more than the ordering block holds, so the iterations take the full sort
+    after the classification has already queued moves; the result is still
+    the oracle's."""
+    g = graphs.grid2d(250, 250, weighted=False).as_tier(tier)
+    og = orc.G.from_csr(g)
+    prev = jet.set_refine_drivers(jet.DRIVER_ALL)
+    try:
+        seen = _skewed_runs(jet, orc, g, og, 8, 1.03, 0.9, iters_list=(1, 2, 3, 4))
+    finally:
+        jet.set_refine_drivers(prev)
+    assert 1 in seen
 
 
 @pytest.mark.parametrize("tier", TIERS)
@@ -318,7 +351,7 @@ def test_edge_cases(jet, graphs, orc):
     assert orc.pstat(orc.G.from_csr(small), p, 3)[0] == cut
 
 
-@pytest.mark.parametrize("drivers", ["all", "cta_global", "cluster", "coop", "graph", "host"])
+@pytest.mark.parametrize("drivers", ["all", "all_fullsort", "cta_global", "cluster", "coop", "graph", "host", "host_fullsort"])
 @pytest.mark.parametrize("tier,kind,k", [("i32", "grid2d", 16), ("big", "rgg", 64), ("biggest", "grid2d", 300),
                                          ("i32", "rgg", 600)])
 def test_level_drivers_bit_exact(jet, graphs, orc, drivers, tier, kind, k):
@@ -326,8 +359,10 @@ def test_level_drivers_bit_exact(jet, graphs, orc, drivers, tier, kind, k):
     memory, one thread-block cluster, cooperative grid kernel, CUDA graph
     with conditional nodes, host loop) returns the oracle's partition on
     graphs whose finer levels exceed the one-CTA bound."""
-    mask = {"all": jet.DRIVER_ALL, "cta_global": jet.DRIVER_CTA, "cluster": jet.DRIVER_CLUSTER, "coop": jet.DRIVER_COOP | jet.DRIVER_GRAPH,
-            "graph": jet.DRIVER_GRAPH, "host": 0}[drivers]
+    q = jet.DRIVER_REB_QUEUE
+    mask = {"all": jet.DRIVER_ALL, "all_fullsort": jet.DRIVER_ALL & ~q, "cta_global": jet.DRIVER_CTA | q,
+            "cluster": jet.DRIVER_CLUSTER | q, "coop": jet.DRIVER_COOP | jet.DRIVER_GRAPH | q, "graph": jet.DRIVER_GRAPH | q,
+            "host": q, "host_fullsort": 0}[drivers]
     g = graphs.grid2d(170, 150, weighted=True, seed=7) if kind == "grid2d" else graphs.rgg(30000, 9.0, seed=5)
     g = g.as_tier(tier)
     og = orc.G.from_csr(g)
@@ -534,15 +569,15 @@ def test_gpu_matches_reference_directly(jet, graphs, orc, ref, tier, kind, k):
 
 
 def test_class_profiling_pass_leaves_results_unchanged(jet, graphs, orc):
-    """The profiling pass (every level on the host-driven loop, event brackets
-    per kernel class, device-side counts for the byte model) returns the same
+    """The profiling pass (every level on the host-driven loop with the
+    rebalance queue, event brackets per kernel class, device-side counts for the byte model) returns the same
     partition as a normal call, and accounts time and bytes to the classes
     that ran."""
     g = graphs.grid3d(40, 40, 30, weighted=True, seed=4)
     og = orc.G.from_csr(g)
     cfg = jet.config_t(coarsening_alg=1, num_parts=16, max_imb_ratio=1.03)
     want, wcut, _ = orc.partition(og, 16, alg=1, imb=1.03, seed=2)
-    prev = jet.set_refine_drivers(0)
+    prev = jet.set_refine_drivers(jet.DRIVER_REB_QUEUE)
     try:
         jet.prof_enable(True)
         part, cut, _ = jet.partition(cfg, g.to("cuda"), seed=2)
