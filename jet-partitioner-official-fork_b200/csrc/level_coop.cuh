@@ -216,7 +216,7 @@ __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>
         volatile RefDev<O, W>* vd = a.dev;
         const O count = vd->nord;
         const int fb = vd->reb_fb || count > (O)cs.qcap;
-        if (!fb && blockIdx.x == 0) d_reb_queue_tail<STRONG, O, E, W>(a, rb, count, (uint64_t*)smem_raw);
+        if (!fb && blockIdx.x == 0) d_reb_queue_tail<STRONG, O, E, W>(a, rb, count, (uint64_t*)smem_raw, cs.qcap, &pc);
         // every block has read the queue state before block 0 resets it
         if (!level_sync<CL>(cs.bar, err)) return false;
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -226,10 +226,7 @@ __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>
             a.dev->reb_fb = 0;
             if (fb) a.dev->nmoves = 0;  // the full sort below decides every move again
         }
-        if (!fb) {
-            pc.mark(PH_REB_EVICT);
-            return true;
-        }
+        if (!fb) return true;
     }
     uint32_t(*cnt)[RS_BINS] = (uint32_t(*)[RS_BINS])smem_raw;  // 32 x 256 counters (dynamic shared memory)
     // stable sort of (bucket id, vertex) pairs

@@ -71,8 +71,7 @@ __device__ __forceinline__ void d_reb_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb,
         __syncthreads();
         pc.mark(PH_REB_SORT);
         if (!s_fb) {
-            d_reb_queue_tail<STRONG, O, E, W>(a, rb, s_count, keys);
-            pc.mark(PH_REB_EVICT);
+            d_reb_queue_tail<STRONG, O, E, W>(a, rb, s_count, keys, P, &pc);
             return;
         }
     }

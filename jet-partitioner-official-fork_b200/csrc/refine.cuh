@@ -1365,19 +1365,22 @@ __device__ __forceinline__ void block_sort_keys(K* key, int P) {
 }
 // The replay is one thread's serial walk (each draw advances the shared
 // cursor), so what it reads is staged first: the chunk bounds in shared
-// memory (when k fits), and each vertex's weight, chunk and part are loaded
-// one vertex ahead of their use.
+// memory (when k fits) and, given `stage` shared memory for it, each queued
+// vertex's weight and chunk, with the chosen chunks written back there and
+// stored by the whole block; without it each vertex's data is loaded one
+// vertex ahead of its use.
 static constexpr int REDRAW_ES_CAP = 513;
 template <class O, class E, class W>
-__device__ __forceinline__ void d_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W> rb) {
+__device__ __forceinline__ void d_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W> rb, unsigned char* stage = nullptr,
+                                                size_t stage_bytes = 0) {
     __shared__ O list[REDRAW_CAP];
     __shared__ W es_s[REDRAW_ES_CAP];
     O cnt = a.dev->nredraw;
     if (cnt == 0) return;
-    const bool stage = a.k + 1 <= REDRAW_ES_CAP;
-    if (stage)
+    const bool es_in = a.k + 1 <= REDRAW_ES_CAP;
+    if (es_in)
         for (int p = threadIdx.x; p <= a.k; p += blockDim.x) es_s[p] = rb.evict_start[p];
-    const W* es = stage ? es_s : rb.evict_start;
+    const W* es = es_in ? es_s : rb.evict_start;
     bool fits = cnt <= REDRAW_CAP;
     if (fits) {
         int P = 1;
@@ -1388,6 +1391,41 @@ __device__ __forceinline__ void d_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W
     } else {
         __syncthreads();
         if (threadIdx.x == 0) atomicOr(&a.dev->err, 16);  // more draws than the replay buffer: order falls back to queue order
+    }
+    if (fits && stage && (size_t)cnt * (sizeof(W) + sizeof(int)) <= stage_bytes) {
+        W* sw = (W*)stage;
+        int* sp = (int*)(stage + (size_t)cnt * sizeof(W));
+        for (int x = threadIdx.x; x < (int)cnt; x += blockDim.x) {
+            const O v = list[x];
+            sw[x] = a.g.vw[v];
+            sp[x] = rb.redraw_p[v];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            W cursor = a.dev->vw_cursor;
+            for (int x = 0; x < (int)cnt; x++) {
+                const W w = sw[x];
+                int p = sp[x];
+                int dest = -1;
+                int guard = 0;
+                while (p < a.k) {
+                    W sc = cursor;
+                    cursor += w;
+                    while (p <= a.k && es[p] <= sc) p++;
+                    p--;
+                    if (p < a.k && w / 2 <= es[p + 1] - sc) { dest = p; break; }
+                    if (++guard > 4 * a.k + 64) { atomicOr(&a.dev->err, ERRF_SPIN); break; }
+                }
+                sp[x] = dest;
+            }
+            a.dev->vw_cursor = cursor;
+        }
+        __syncthreads();
+        for (int x = threadIdx.x; x < (int)cnt; x += blockDim.x) {
+            const O v = list[x];
+            a.dest[v] = sp[x] >= 0 ? (part_t)sp[x] : a.part[v];
+        }
+        return;
     }
     if (threadIdx.x != 0) return;
     W cursor = a.dev->vw_cursor;
@@ -1571,17 +1609,23 @@ __device__ __forceinline__ void d_reb_ordered(RefArgs<O, E, W> a, RebArgs<O, W> 
 }
 
 // The ordered eviction and, for strong rebalancing, the cookie cutter and the
-// destination draws, all in one block.
+// destination draws, all in one block.  keys: key_cap 64-bit entries of
+// shared memory (at least count), reused by the draws once the order is done.
 template <bool STRONG, class O, class E, class W>
-__device__ __forceinline__ void d_reb_queue_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb, O count, uint64_t* keys) {
+__device__ __forceinline__ void d_reb_queue_tail(RefArgs<O, E, W> a, RebArgs<O, W> rb, O count, uint64_t* keys, int key_cap,
+                                                 PhaseClock* pc) {
     d_reb_ordered<STRONG, O, E, W>(a, rb, count, keys);
+    if (pc) pc->mark(PH_REB_EVICT);
     if (STRONG) {
         d_cookie<O, E, W>(a, rb);
         __syncthreads();
+        if (pc) pc->mark(PH_COOKIE);
         d_strong_first<O, E, W>(a, rb, threadIdx.x, blockDim.x);
         __syncthreads();
-        d_strong_redraw<O, E, W>(a, rb);
+        if (pc) pc->mark(PH_STRONG_FIRST);
+        d_strong_redraw<O, E, W>(a, rb, (unsigned char*)keys, (size_t)key_cap * sizeof(uint64_t));
         __syncthreads();
+        if (pc) pc->mark(PH_REDRAW);
     }
 }
 
@@ -1618,7 +1662,7 @@ __global__ void __launch_bounds__(1024) k_reb_ordered(RefArgs<O, E, W> a, RebArg
     }
     __syncthreads();
     if (s_fb) return;
-    d_reb_queue_tail<STRONG, O, E, W>(a, rb, s_count, (uint64_t*)smem_raw);
+    d_reb_queue_tail<STRONG, O, E, W>(a, rb, s_count, (uint64_t*)smem_raw, cap, nullptr);
 }
 
 // ---------------------------------------------------------------- moves
