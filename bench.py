@@ -289,15 +289,6 @@ def run_only(args, wl, local):
     torch.cuda.set_device(local)
     jet = load_pkg()
     dev = torch.device("cuda", local)
-    if args.serving_only:
-        # the serving config on its own: one JSON line with the stream's
-        # capacity and its p50/p99 latency under Poisson arrivals
-        t0 = time.perf_counter()
-        sv = run_serving(jet, dev, args.serving, args.workers, 120 << 30, nmax=args.serving_nmax,
-                         pool=args.serving_pool, rates=[float(x) for x in args.serving_rates.split(",") if x])
-        print(json.dumps({"metric": "graphs/sec (serving)", "value": sv["all_at_once"]["graphs_per_s"], "unit": "graphs/s",
-                          "n_gpus": 1, "data": "synthetic", "wall_s": time.perf_counter() - t0, "serving": sv}), flush=True)
-        return
     g = wl["make"](jet.graphs, dev)
     k = wl["k"]
     level = 1

@@ -2,6 +2,7 @@
 // the uncoarsening loop (src/uncoarsen.hpp:88-158) and the whole partition
 // (src/partitioner.hpp:61-125).
 #pragma once
+#include <cstdlib>
 #include "partitioner.cuh"
 #include "sort.cuh"
 #include "level_coop.cuh"
@@ -760,8 +761,19 @@ struct Refiner {
     // workers keep one CTA up to CTA_MAX_N: with many partitions sharing the
     // GPU, one SM per level gives more throughput than sixteen.
     static constexpr int64_t CTA_PREFER_N = 2048;
+    // The drivers' size bounds, each overridable once per process by an
+    // environment variable of the same name with a JET_ prefix (for tuning
+    // on other parts; the defaults are the measured crossovers on B200).
+    static int64_t bound(const char* env, int64_t def) {
+        const char* v = std::getenv(env);
+        return (v && *v) ? std::atoll(v) : def;
+    }
+    static int64_t cta_prefer_n() { static const int64_t v = bound("JET_CTA_PREFER_N", CTA_PREFER_N); return v; }
+    static int64_t cluster_max_n() { static const int64_t v = bound("JET_CLUSTER_MAX_N", CLUSTER_MAX_N); return v; }
+    static int64_t coop_max_n() { static const int64_t v = bound("JET_COOP_MAX_N", COOP_MAX_N); return v; }
+    static int64_t persistent_max_m() { static const int64_t v = bound("JET_PERSISTENT_MAX_M", CLUSTER_MAX_M); return v; }
     bool cta_eligible(const Level<O, E, W>& L) const {
-        int64_t cap = (use_cluster && !batch_thread() && cluster_size() > 0) ? CTA_PREFER_N : CTA_MAX_N;
+        int64_t cap = (use_cluster && !batch_thread() && cluster_size() > 0) ? cta_prefer_n() : CTA_MAX_N;
         return use_cta && (int64_t)L.n <= cap && (int64_t)L.m <= CTA_MAX_M && k <= CTA_MAX_K;
     }
 
@@ -835,8 +847,8 @@ struct Refiner {
         return bytes;
     }
     bool coop_eligible(const Level<O, E, W>& L) const {
-        return use_coop && device_info().coop && !cta_eligible(L) && (int64_t)L.n <= COOP_MAX_N &&
-               (int64_t)L.m <= CLUSTER_MAX_M && k <= WARP_TABLE &&
+        return use_coop && device_info().coop && !cta_eligible(L) && (int64_t)L.n <= coop_max_n() &&
+               (int64_t)L.m <= persistent_max_m() && k <= WARP_TABLE &&
                coop_smem() + coop_static_smem() <= (size_t)device_info().max_smem_optin;
     }
 
@@ -876,7 +888,7 @@ struct Refiner {
         return cluster_cache;
     }
     bool cluster_eligible(const Level<O, E, W>& L) const {
-        return use_cluster && !cta_eligible(L) && (int64_t)L.n <= CLUSTER_MAX_N && (int64_t)L.m <= CLUSTER_MAX_M &&
+        return use_cluster && !cta_eligible(L) && (int64_t)L.n <= cluster_max_n() && (int64_t)L.m <= persistent_max_m() &&
                k <= WARP_TABLE &&
                coop_smem() + coop_static_smem() <= (size_t)device_info().max_smem_optin && cluster_size() > 0;
     }
