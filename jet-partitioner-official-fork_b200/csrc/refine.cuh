@@ -1363,6 +1363,22 @@ __device__ __forceinline__ void block_sort_keys(K* key, int P) {
         }
     }
 }
+// The chunk scan of the destination draw (src/jet_refiner.hpp:529-531):
+// from p, step while es[p] <= sc, then step back one.  es is a prefix of
+// non-negative capacities (non-decreasing), so the first index past p whose
+// bound exceeds sc is found by a binary search; the result is the scan's.
+template <class W>
+__device__ __forceinline__ int chunk_scan(const W* es, int p, int k, W sc) {
+    if (p > k || es[p] > sc) return p - 1;
+    int lo = p + 1, hi = k + 1;  // es[lo - 1] <= sc; find the first q in [lo, k] with es[q] > sc, else k + 1
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (es[mid] <= sc) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo - 1;
+}
+
 // The replay is one thread's serial walk (each draw advances the shared
 // cursor), so what it reads is staged first: the chunk bounds in shared
 // memory (when k fits) and, given `stage` shared memory for it, each queued
@@ -1411,8 +1427,7 @@ __device__ __forceinline__ void d_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W
                 while (p < a.k) {
                     W sc = cursor;
                     cursor += w;
-                    while (p <= a.k && es[p] <= sc) p++;
-                    p--;
+                    p = chunk_scan<W>(es, p, a.k, sc);
                     if (p < a.k && w / 2 <= es[p + 1] - sc) { dest = p; break; }
                     if (++guard > 4 * a.k + 64) { atomicOr(&a.dev->err, ERRF_SPIN); break; }
                 }
@@ -1449,8 +1464,7 @@ __device__ __forceinline__ void d_strong_redraw(RefArgs<O, E, W> a, RebArgs<O, W
         while (p < a.k) {
             W sc = cursor;
             cursor += w;
-            while (p <= a.k && es[p] <= sc) p++;
-            p--;
+            p = chunk_scan<W>(es, p, a.k, sc);
             if (p < a.k && w / 2 <= es[p + 1] - sc) { dest = p; break; }
             if (++guard > 4 * a.k + 64) { atomicOr(&a.dev->err, ERRF_SPIN); break; }
         }
