@@ -196,6 +196,7 @@ struct CoopScratch {
     W* wpre;             // prefix of candidate weights in sorted order (n)
     O* marked;           // rows to rebuild after a large move set (n)
     int qcap;            // queued candidates block 0 can order in its dynamic shared memory
+    int64_t boff_cap;    // bucket offsets each block can keep in shared memory past the keys (0: none)
 };
 
 // Rebalance tail over the grid (sort_candidates + k_evict_sorted [+ strong]).
@@ -203,10 +204,20 @@ template <bool CL, bool STRONG, class O, class E, class W>
 __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>& rb, CoopScratch<O, E, W>& cs, int bits,
                                               PhaseClock& pc) {
     int* err = &a.dev->err;
-    if (!grid_scan<CL, W>(GetArray<W>{rb.buckets}, (int64_t)rb.t_minibuckets + 1, rb.boff, cs.wsum, cs.bar, err)) return false;
-    pc.mark(PH_REB_SCAN);
     const int64_t n = a.g.n;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    if ((int64_t)rb.t_minibuckets + 1 <= cs.boff_cap) {
+        // every block scans the bucket totals into its own shared copy of the
+        // offsets (no grid barrier); all later readers in this rebalance
+        // (classification, ordering, eviction, cookie cutter, destinations)
+        // read the copy of their own block
+        W* boff_s = (W*)(smem_raw + (size_t)cs.qcap * sizeof(uint64_t));
+        block_scan_global<W>(rb.buckets, boff_s, (int64_t)rb.t_minibuckets + 1);
+        rb.boff = boff_s;
+    } else if (!grid_scan<CL, W>(GetArray<W>{rb.buckets}, (int64_t)rb.t_minibuckets + 1, rb.boff, cs.wsum, cs.bar, err)) {
+        return false;
+    }
+    pc.mark(PH_REB_SCAN);
     if (rb.queue) {
         // the grid classifies; block 0 orders the queue (when it fits) and
         // finishes the rebalance while the other blocks wait at the barrier

@@ -27,18 +27,23 @@ struct LevelLists {
     int group;
 };
 
-// Exclusive scan of in[0..n) into out (may alias), over the block.
+// Exclusive scan of in[0..n) into out (may alias), over the block: each
+// thread sums a contiguous run, one block scan of the run sums, then each
+// thread writes its run's prefixes (one barrier round for any n).
 template <class T>
 __device__ __forceinline__ void block_scan_global(const T* in, T* out, int64_t n) {
     __shared__ T sw[32];
-    T carry = 0;
-    for (int64_t base = 0; base < n; base += blockDim.x) {
-        int64_t i = base + threadIdx.x;
-        T v = i < n ? in[i] : T(0);
-        T tot;
-        T ex = block_exclusive_scan<T>(v, sw, tot);
-        if (i < n) out[i] = carry + ex;
-        carry += tot;
+    const int64_t per = (n + blockDim.x - 1) / blockDim.x;
+    const int64_t lo = (int64_t)threadIdx.x * per;
+    const int64_t hi = lo + per < n ? lo + per : n;
+    T s = 0;
+    for (int64_t i = lo; i < hi; i++) s += in[i];
+    T tot;
+    T ex = block_exclusive_scan<T>(s, sw, tot);
+    for (int64_t i = lo; i < hi; i++) {
+        const T v = in[i];
+        out[i] = ex;
+        ex += v;
     }
     __syncthreads();
 }

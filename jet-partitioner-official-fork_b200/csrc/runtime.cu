@@ -611,8 +611,9 @@ int jet_set_refine_drivers(int mask) { return g_drivers.exchange(mask & JET_DRIV
 // spinning and send Metis calls to helper processes.
 void jet_thread_batch_mode(int on) {
     // one CTA for small levels, a 16-CTA cluster for mid-size ones (it needs
-    // 16 SMs, not the whole GPU), the host loop above
-    t_driver_mask = on ? (JET_DRIVER_CTA | JET_DRIVER_CLUSTER) : JET_DRIVER_ALL;
+    // 16 SMs, not the whole GPU), the host loop above; the loops' options
+    // (state in shared memory, the rebalance queue) as everywhere else
+    t_driver_mask = on ? (JET_DRIVER_CTA | JET_DRIVER_CLUSTER | JET_DRIVER_CTA_SMEM | JET_DRIVER_REB_QUEUE) : JET_DRIVER_ALL;
     t_batch = on != 0;
 }
 

@@ -769,7 +769,12 @@ struct Refiner {
         return (v && *v) ? std::atoll(v) : def;
     }
     static int64_t cta_prefer_n() { static const int64_t v = bound("JET_CTA_PREFER_N", CTA_PREFER_N); return v; }
-    static int64_t cluster_max_n() { static const int64_t v = bound("JET_CLUSTER_MAX_N", CLUSTER_MAX_N); return v; }
+    static int64_t cluster_max_n() {
+        // batch and server workers share the GPU: their bound is separate
+        static const int64_t v = bound("JET_CLUSTER_MAX_N", CLUSTER_MAX_N);
+        static const int64_t vb = bound("JET_BATCH_CLUSTER_MAX_N", CLUSTER_MAX_N);
+        return batch_thread() ? vb : v;
+    }
     static int64_t coop_max_n() { static const int64_t v = bound("JET_COOP_MAX_N", COOP_MAX_N); return v; }
     static int64_t persistent_max_m() { static const int64_t v = bound("JET_PERSISTENT_MAX_M", CLUSTER_MAX_M); return v; }
     bool cta_eligible(const Level<O, E, W>& L) const {
@@ -832,13 +837,25 @@ struct Refiner {
         size_t nw = CTA_THREADS / 32;
         size_t conn = ((nw * kw * sizeof(part_t) + 15) & ~(size_t)15) + nw * kw * sizeof(W);
         size_t rs = (size_t)32 * RS_BINS * sizeof(uint32_t);
-        size_t q = (size_t)COOP_QUEUE_KEYS * sizeof(uint64_t);
+        size_t q = (size_t)COOP_QUEUE_KEYS * sizeof(uint64_t) + (size_t)coop_boff_cap() * sizeof(W);
         size_t b = conn > rs ? conn : rs;
         return (b > q ? b : q) + 64;
     }
     // rebalance candidates block 0 of the persistent grid orders in shared memory
     static constexpr int COOP_QUEUE_KEYS = 8192;
-    int coop_qcap() const { return (int)((coop_smem() - 64) / sizeof(uint64_t)); }
+    int coop_qcap() const { return COOP_QUEUE_KEYS; }
+    // bucket offsets every block of the persistent grid keeps in shared
+    // memory after the keys: room for the largest level the grid drivers
+    // take, within 128 KiB (else those levels scan them across the grid)
+    int64_t coop_boff_cap() const {
+        int64_t nmax = (int64_t)n_max;
+        const int64_t lim = coop_max_n() > cluster_max_n() ? coop_max_n() : cluster_max_n();
+        if (nmax > lim) nmax = lim;
+        O sections, tmb;
+        sections_for((O)nmax, sections, tmb);
+        const int64_t want = (int64_t)tmb + 1;
+        return want * (int64_t)sizeof(W) <= ((int64_t)128 << 10) ? want : 0;
+    }
     size_t coop_static_smem() const {
         static size_t bytes = [] {
             cudaFuncAttributes fa;
@@ -919,7 +936,8 @@ struct Refiner {
         LevelLists<O> li{L.warp_list.p, L.n_warp, L.hub_list.p, L.n_hub, L.group};
         RebArgs<O, W> rbw = reb_args(L, weak_max_dest(pb.size_max), pb.opt, pb.size_max, false);
         RebArgs<O, W> rbs = reb_args(L, strong_max_dest(pb.opt, pb.size_max), pb.opt, pb.size_max, false);
-        CoopScratch<O, E, W> cs{cbar.p, cwsum.p, chist.p, sk0.p, sk1.p, sv0.p, sv1.p, wpre.p, cmarked.p, coop_qcap()};
+        CoopScratch<O, E, W> cs{cbar.p, cwsum.p, chist.p, sk0.p, sk1.p, sv0.p, sv1.p, wpre.p, cmarked.p, coop_qcap(),
+                                coop_boff_cap()};
         int bits = bits_for((uint64_t)rbw.none_key);
         int max_iters = 1 << 22;
         RefArgs<O, E, W> a = args(L);
