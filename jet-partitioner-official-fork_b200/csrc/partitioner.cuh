@@ -37,6 +37,12 @@ struct Engine {
     IterResult* hres = nullptr;
     int slot0 = -1;
 
+    // side streams for the independent contraction bins of large levels
+    // (made on first use), with the fork and join events
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[3] = {nullptr, nullptr, nullptr};
+
     explicit Engine(cudaStream_t st) : s(st) {
         dscal.alloc(64, s);
         slot0 = pinned_acquire(64 * sizeof(int64_t) + sizeof(IterResult) + 64);
@@ -45,7 +51,21 @@ struct Engine {
     }
     ~Engine() {
         cudaStreamSynchronize(s);
+        for (int i = 0; i < 3; i++) {
+            if (side[i]) { cudaStreamSynchronize(side[i]); cudaStreamDestroy(side[i]); }
+            if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
         pinned_release(slot0);
+    }
+    bool side_streams() {
+        if (ev_fork) return true;
+        for (int i = 0; i < 3; i++) {
+            if (cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&ev_join[i], cudaEventDisableTiming) != cudaSuccess)
+                return false;
+        }
+        return cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming) == cudaSuccess;
     }
     template <class T> T* dslot(int i) { return (T*)(dscal.p + i); }
     void sync() { stream_wait(s); }
@@ -372,6 +392,7 @@ struct Engine {
         return (int64_t)*(W*)hscal < ((int64_t)1 << 31) ? 1 : 0;
     }
     // build_coarse_graph, src/contract.hpp:347-446.
+    static constexpr int64_t CONTRACT_FORK_M = (int64_t)1 << 22;
     void contract(const Level<O, E, W>& L, const O* map, O nc, Level<O, E, W>& C, DBuf<O>* skey_buf, DBuf<W>* sval_buf) {
         if (narrow_w < 0) narrow_w = weight_fits_32(L);
         auto g = L.view();
@@ -412,6 +433,33 @@ struct Engine {
         k_contract_bin<O, E><<<grid_persistent(nc, 8), BLOCK, 0, s>>>(nc, hrow.p, l1.p, n1, l2a.p, n2a, l2b.p, n2b, l2.p, n2, lh.p, nh);
         count_launch();
         JET_LAUNCH_CHECK();
+        // The bins write disjoint rows: on a large level they run side by side
+        // (the warp bin and the hub rows on this stream, the shared-memory
+        // bins on three side streams), so that one bin's tail overlaps the
+        // others' work.  Batch workers keep one stream each.
+        const bool fork = (int64_t)L.m >= CONTRACT_FORK_M && !batch_thread() && !capturing() && side_streams();
+        cudaStream_t sa = s, sb = s, sc = s;
+        // joins the side streams back into s on every way out of this
+        // function (an exception included) before the bins' buffers are freed
+        struct Join {
+            Engine* e;
+            bool on;
+            ~Join() {
+                if (!on) return;
+                for (int i = 0; i < 3; i++) {
+                    cudaEventRecord(e->ev_join[i], e->side[i]);
+                    cudaStreamWaitEvent(e->s, e->ev_join[i], 0);
+                }
+            }
+        } join{this, false};
+        if (fork) {
+            JET_CUDA(cudaEventRecord(ev_fork, s));
+            for (int i = 0; i < 3; i++) JET_CUDA(cudaStreamWaitEvent(side[i], ev_fork, 0));
+            join.on = true;
+            sa = side[0];
+            sb = side[1];
+            sc = side[2];
+        }
         k_contract_warp<O, E, W><<<grid_persistent((int64_t)nc * 32, 16), BLOCK, 0, s>>>(g, map, nc, moff.p, members.p, hrow.p, skey, sval, ucnt.p); count_launch();
         JET_LAUNCH_CHECK();
         {
@@ -423,21 +471,23 @@ struct Engine {
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
             JET_CUDA(cudaFuncSetAttribute(k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2a));
-            k_contract_smem<CT_S1_THREADS, CT_S1_SLOTS, O, E, W><<<device_info().sms * 8, CT_S1_THREADS, sm1, s>>>(
+            int per_sm = 0;
+            JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contract_smem<CT_S1_THREADS, CT_S1_SLOTS, O, E, W>,
+                                                                   CT_S1_THREADS, sm1));
+            k_contract_smem<CT_S1_THREADS, CT_S1_SLOTS, O, E, W><<<device_info().sms * (per_sm > 0 ? per_sm : 1), CT_S1_THREADS, sm1, sa>>>(
                 g, map, l1.p, n1, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc, narrow_w); count_launch();
             JET_LAUNCH_CHECK();
-            int per_sm = 0;
             JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W>,
                                                                    CT_S2A_THREADS, sm2a));
-            k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W><<<device_info().sms * (per_sm > 0 ? per_sm : 1), CT_S2A_THREADS, sm2a, s>>>(
+            k_contract_smem<CT_S2A_THREADS, CT_S2A_SLOTS, O, E, W><<<device_info().sms * (per_sm > 0 ? per_sm : 1), CT_S2A_THREADS, sm2a, sb>>>(
                 g, map, l2a.p, n2a, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc, narrow_w); count_launch();
             JET_LAUNCH_CHECK();
             JET_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_contract_smem<CT_S2B_THREADS, CT_S2B_SLOTS, O, E, W>,
                                                                    CT_S2B_THREADS, sm2b));
-            k_contract_smem<CT_S2B_THREADS, CT_S2B_SLOTS, O, E, W><<<device_info().sms * (per_sm > 0 ? per_sm : 1), CT_S2B_THREADS, sm2b, s>>>(
+            k_contract_smem<CT_S2B_THREADS, CT_S2B_SLOTS, O, E, W><<<device_info().sms * (per_sm > 0 ? per_sm : 1), CT_S2B_THREADS, sm2b, sc>>>(
                 g, map, l2b.p, n2b, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc, narrow_w); count_launch();
             JET_LAUNCH_CHECK();
-            k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W><<<device_info().sms * 2, CT_S2_THREADS, sm2, s>>>(
+            k_contract_smem<CT_S2_THREADS, CT_S2_SLOTS, O, E, W><<<device_info().sms * 2, CT_S2_THREADS, sm2, sb>>>(
                 g, map, l2.p, n2, moff.p, members.p, hrow.p, skey, sval, ucnt.p, nc, narrow_w); count_launch();
             JET_LAUNCH_CHECK();
             if (dense) {
@@ -446,6 +496,13 @@ struct Engine {
                 JET_LAUNCH_CHECK();
             } else {
                 contract_hubs_sorted(g, map, lh.p, nh, moff.p, members.p, hrow.p, nc, skey, sval, ucnt.p);
+            }
+        }
+        if (fork) {
+            join.on = false;
+            for (int i = 0; i < 3; i++) {
+                JET_CUDA(cudaEventRecord(ev_join[i], side[i]));
+                JET_CUDA(cudaStreamWaitEvent(s, ev_join[i], 0));
             }
         }
         // coarse row offsets and nnz
