@@ -20,7 +20,7 @@ struct GridBar {
     unsigned int count;
     unsigned int gen;
     int abort;
-    int pad;
+    unsigned int cut_done;       // blocks done with the cut change this iteration
     int64_t nmarked;             // rows queued for rebuild this iteration
 };
 
@@ -298,7 +298,6 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl_begin_logic(c);
     if (!level_sync<CL>(cs.bar, err)) return;
     PhaseClock pc(a.pclk, CL ? 2 * PHASE_SLOTS : 4 * PHASE_SLOTS, blockIdx.x == 0 && threadIdx.x == 0);
-    int iters = 0;
     while (true) {
         const int more = ((volatile Ctl<W>*)c)->more;
         const int mode = ((volatile Ctl<W>*)c)->mode;
@@ -317,9 +316,11 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
             }
             if (!level_sync<CL>(cs.bar, err)) return;
             pc.mark(PH_AFTERBURN);
-            d_afterburn_hub<O, E, W>(a);
-            if (!level_sync<CL>(cs.bar, err)) return;
-            pc.mark(PH_AFTERBURN_HUB);
+            if (li.n_hub > 0) {
+                d_afterburn_hub<O, E, W>(a);
+                if (!level_sync<CL>(cs.bar, err)) return;
+                pc.mark(PH_AFTERBURN_HUB);
+            }
         } else {
             RebArgs<O, W>& rb = mode == MODE_WEAK ? rbw : rbs;
             // bucket totals cleared while block 0 lists the parts (neither
@@ -384,24 +385,38 @@ k_level_coop(RefArgs<O, E, W> a, LevelLists<O> li, RebArgs<O, W> rbw, RebArgs<O,
         }
         pc.mark(PH_REBUILD);
         d_cut_after<O, E, W>(a);
-        if (!level_sync<CL>(cs.bar, err)) return;
-        pc.mark(PH_CUT);
-        if (blockIdx.x == 0) {
-            W mx = block_max_sizes<W>(a.sizes, a.k);
+        // the last block to finish its share of the cut change closes the
+        // iteration (one barrier instead of two): its fence and counter add
+        // come after every other block's cut atomics
+        {
+            __shared__ int s_last;
+            __syncthreads();
             if (threadIdx.x == 0) {
-                ctl_end_logic<O, W>(c, a.dev, mx);
-                cs.bar->nmarked = 0;
-                if (c->more && ++iters >= max_iters) { c->more = 0; atomicOr(err, ERRF_SPIN); }
+                __threadfence();
+                s_last = atomicAdd(&cs.bar->cut_done, 1u) == gridDim.x - 1;
+            }
+            __syncthreads();
+            if (s_last) {
+                __threadfence();
+                W mx = block_max_sizes<W>(a.sizes, a.k);
+                if (threadIdx.x == 0) {
+                    cs.bar->cut_done = 0;
+                    ctl_end_logic<O, W>(c, a.dev, mx);
+                    cs.bar->nmarked = 0;
+                    if (c->more && c->iter_count >= max_iters) { c->more = 0; atomicOr(err, ERRF_SPIN); }
+                }
             }
         }
         if (!level_sync<CL>(cs.bar, err)) return;
-        pc.mark(PH_CTL);
+        pc.mark(PH_CUT);
+        // the copy of the best state needs no barrier of its own: what it
+        // reads (parts, sizes) is next written by the apply phase, at least
+        // one barrier later, and nothing reads what it writes during the loop
         if (((volatile Ctl<W>*)c)->copy) {
             for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
                 best_part[i] = a.part[i];
             for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < a.k; p += gridDim.x * blockDim.x) sizes_best[p] = a.sizes[p];
         }
-        if (!level_sync<CL>(cs.bar, err)) return;
         pc.mark(PH_COPY);
     }
     pc.flush();

@@ -549,11 +549,12 @@ struct Refiner {
         const double so = sizeof(O), se = sizeof(E), sw = sizeof(W), sl = sizeof(Slot<W>);
         const double n = (double)L.n, T = (double)c.moves, Td = (double)c.moves_deg;
         if (kind == 0) {
-            // LP select: cache test and destination write for every vertex;
-            // the uncached ones read part, offset, size and their table and
-            // write gain and cache; candidates are appended
-            prof_add_bytes(ph[PK_LP_SELECT], n * (4 + 4) + (double)c.uncached * (4 + se + 4 + sw + 4) +
-                                                 (double)c.size_uncached * sl + (double)c.cand * so);
+            // LP select: for every vertex its row offset (degree class),
+            // cache test, destination write, lock and pre-gain; the uncached
+            // ones read part, offset, size and their table and write gain and
+            // cache; candidates read their saved gain and are appended
+            prof_add_bytes(ph[PK_LP_SELECT], n * (se + 4 + 4 + 1 + sw) + (double)c.uncached * (4 + se + 4 + sw + 4) +
+                                                 (double)c.size_uncached * sl + (double)c.cand * (sw + so));
             // afterburner: each candidate's row, pregain, part and destination;
             // per edge the neighbour, weight and the neighbour's pregain,
             // destination and part; the kept ones are locked and appended
