@@ -22,6 +22,22 @@ struct Slot {
     W v;
 };
 
+// Visits slots [0, sz) of a table in order, loading four at a time before
+// the first use: a one-thread scan of a row's table is a chain of dependent
+// waits otherwise (each use stalls the next load's issue).
+template <class W, class F>
+__device__ __forceinline__ void scan_slots(const Slot<W>* base, part_t sz, F&& body) {
+    for (part_t s0 = 0; s0 < sz; s0 += 4) {
+        Slot<W> sl[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (s0 + u < sz) sl[u] = base[s0 + u];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (s0 + u < sz) body(sl[u]);
+    }
+}
+
 // Home slot of part p in a table of `size` slots: p itself when the table is
 // direct-mapped (size == k), else a multiplicative hash scaled to the size
 // (no division).  Only the slot layout depends on this choice, never a
@@ -779,11 +795,10 @@ __device__ __forceinline__ void d_lp_select_thread(RefArgs<O, E, W> a) {
                 W b_conn = 0, p_conn = 0;
                 const Slot<W>* base = a.slots + a.coff[i];
                 part_t sz = a.csize[i];
-                for (part_t s = 0; s < sz; s++) {
-                    Slot<W> sl = base[s];
+                scan_slots<W>(base, sz, [&](const Slot<W>& sl) {
                     if (sl.p != p) { if (lp_better<W>(sl.v, sl.p, b_conn, best)) { best = sl.p; b_conn = sl.v; } }
                     else if (sl.v > 0) p_conn = sl.v;
-                }
+                });
                 lp_finish<O, E, W>(a, i, best, b_conn, p_conn, filter_ratio, true);
                 best = a.dest[i];
             }
@@ -1077,13 +1092,12 @@ __device__ __forceinline__ void d_weak_select_thread(RefArgs<O, E, W> a, RebArgs
         if (elig) {
             const Slot<W>* base = a.slots + a.coff[i];
             part_t sz = a.csize[i];
-            for (part_t s = 0; s < sz; s++) {
-                Slot<W> sl = base[s];
+            scan_slots<W>(base, sz, [&](const Slot<W>& sl) {
                 if (sl.p > NULL_PART && a.sizes[sl.p] < rb.max_dest) {
                     if (sl.v > gain || (sl.v == gain && sl.v > 0 && sl.p < best)) { best = sl.p; gain = sl.v; }
                 }
                 if (sl.p == p) p_gain = sl.v;
-            }
+            });
         }
         weak_score<O, E, W>(a, rb, i, p, best, gain, p_gain, elig);
     }
@@ -1193,11 +1207,10 @@ __device__ __forceinline__ void d_strong_score_thread(RefArgs<O, E, W> a, RebArg
         W p_gain = 0;
         const Slot<W>* base = a.slots + a.coff[i];
         part_t sz = a.csize[i];
-        for (part_t s = 0; s < sz; s++) {
-            Slot<W> sl = base[s];
+        scan_slots<W>(base, sz, [&](const Slot<W>& sl) {
             if (sl.p == p) p_gain = sl.v;
             else if (sl.p > NULL_PART && a.sizes[sl.p] < rb.max_dest) { tg += (uint64_t)sl.v; tk += 1; }
-        }
+        });
         strong_score<O, E, W>(a, rb, i, p, tg, tk, p_gain);
     }
 }
