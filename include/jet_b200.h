@@ -330,7 +330,7 @@ void jet_free_host(void* ptr);
  * A level uses the first allowed of: one CTA (n <= 2048, or <= 16384 when
  * clusters are not allowed; nnz <= 262144; k <= 256), one thread-block
  * cluster of 8-16 CTAs (n <= 65536, nnz <= 2^21, k <= 512), one cooperative
- * grid kernel (n <= 131072, nnz <= 2^21, k <= 512), a CUDA graph with
+ * grid kernel (n <= 262144, nnz <= 2^22, k <= 512), a CUDA graph with
  * conditional nodes, else the host loop.  JET_DRIVER_CTA_SMEM lets the
  * one-CTA loop keep the level's mutable state in shared memory (as much of
  * it as fits); without it that state stays in global memory.

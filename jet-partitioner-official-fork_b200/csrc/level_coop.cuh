@@ -196,7 +196,8 @@ struct CoopScratch {
     W* wpre;             // prefix of candidate weights in sorted order (n)
     O* marked;           // rows to rebuild after a large move set (n)
     int qcap;            // queued candidates block 0 can order in its dynamic shared memory
-    int64_t boff_cap;    // bucket offsets each block can keep in shared memory past the keys (0: none)
+    int64_t boff_cap;    // bucket offsets each block can keep in shared memory (0: none)
+    int64_t boff_off;    // their byte offset: past the queue keys and the radix counters
 };
 
 // Rebalance tail over the grid (sort_candidates + k_evict_sorted [+ strong]).
@@ -211,7 +212,7 @@ __device__ __forceinline__ bool coop_reb_tail(RefArgs<O, E, W>& a, RebArgs<O, W>
         // offsets (no grid barrier); all later readers in this rebalance
         // (classification, ordering, eviction, cookie cutter, destinations)
         // read the copy of their own block
-        W* boff_s = (W*)(smem_raw + (size_t)cs.qcap * sizeof(uint64_t));
+        W* boff_s = (W*)(smem_raw + cs.boff_off);
         block_scan_global<W>(rb.buckets, boff_s, (int64_t)rb.t_minibuckets + 1);
         rb.boff = boff_s;
     } else if (!grid_scan<CL, W>(GetArray<W>{rb.buckets}, (int64_t)rb.t_minibuckets + 1, rb.boff, cs.wsum, cs.bar, err)) {

@@ -777,7 +777,8 @@ struct Refiner {
         return batch_thread() ? vb : v;
     }
     static int64_t coop_max_n() { static const int64_t v = bound("JET_COOP_MAX_N", COOP_MAX_N); return v; }
-    static int64_t persistent_max_m() { static const int64_t v = bound("JET_PERSISTENT_MAX_M", CLUSTER_MAX_M); return v; }
+    static int64_t cluster_max_m() { static const int64_t v = bound("JET_PERSISTENT_MAX_M", CLUSTER_MAX_M); return v; }
+    static int64_t coop_max_m() { static const int64_t v = bound("JET_PERSISTENT_MAX_M", COOP_MAX_M); return v; }
     bool cta_eligible(const Level<O, E, W>& L) const {
         int64_t cap = (use_cluster && !batch_thread() && cluster_size() > 0) ? cta_prefer_n() : CTA_MAX_N;
         return use_cta && (int64_t)L.n <= cap && (int64_t)L.m <= CTA_MAX_M && k <= CTA_MAX_K;
@@ -832,18 +833,30 @@ struct Refiner {
     }
 
     // ------------------------------------------------------------ cooperative loop
-    static constexpr int64_t COOP_MAX_N = (int64_t)1 << 17;  // above this the multi-kernel graph is faster
+    // Above these the multi-kernel graph is faster (128^3 mesh: the 241,769-
+    // vertex level, 3.1 M entries, runs 86 against 111 us per iteration here;
+    // the 749,582-vertex level gains nothing and the 2 M one loses).
+    static constexpr int64_t COOP_MAX_N = (int64_t)1 << 18;
+    static constexpr int64_t COOP_MAX_M = (int64_t)1 << 22;
     size_t coop_smem() const {
         int kw = k < WARP_TABLE ? k : WARP_TABLE;
         size_t nw = CTA_THREADS / 32;
         size_t conn = ((nw * kw * sizeof(part_t) + 15) & ~(size_t)15) + nw * kw * sizeof(W);
+        size_t q = (size_t)coop_boff_off() + (size_t)coop_boff_cap() * sizeof(W);
+        return (conn > q ? conn : q) + 64;
+    }
+    // the per-block bucket offsets sit past both the queue keys and the full
+    // sort's radix counters (32 warps x 256 digits), which share offset 0
+    static size_t coop_boff_off() {
+        size_t keys = (size_t)COOP_QUEUE_KEYS * sizeof(uint64_t);
         size_t rs = (size_t)32 * RS_BINS * sizeof(uint32_t);
-        size_t q = (size_t)COOP_QUEUE_KEYS * sizeof(uint64_t) + (size_t)coop_boff_cap() * sizeof(W);
-        size_t b = conn > rs ? conn : rs;
-        return (b > q ? b : q) + 64;
+        return ((keys > rs ? keys : rs) + 15) & ~(size_t)15;
     }
     // rebalance candidates block 0 of the persistent grid orders in shared memory
-    static constexpr int COOP_QUEUE_KEYS = 8192;
+    // (2048 keys hold every queue seen on meshes and geometric graphs at
+    // these sizes; more shared memory here would come out of the L1 cache
+    // the loop's global accesses hit)
+    static constexpr int COOP_QUEUE_KEYS = 2048;
     int coop_qcap() const { return COOP_QUEUE_KEYS; }
     // bucket offsets every block of the persistent grid keeps in shared
     // memory after the keys: room for the largest level the grid drivers
@@ -866,7 +879,7 @@ struct Refiner {
     }
     bool coop_eligible(const Level<O, E, W>& L) const {
         return use_coop && device_info().coop && !cta_eligible(L) && (int64_t)L.n <= coop_max_n() &&
-               (int64_t)L.m <= persistent_max_m() && k <= WARP_TABLE &&
+               (int64_t)L.m <= coop_max_m() && k <= WARP_TABLE &&
                coop_smem() + coop_static_smem() <= (size_t)device_info().max_smem_optin;
     }
 
@@ -906,7 +919,7 @@ struct Refiner {
         return cluster_cache;
     }
     bool cluster_eligible(const Level<O, E, W>& L) const {
-        return use_cluster && !cta_eligible(L) && (int64_t)L.n <= cluster_max_n() && (int64_t)L.m <= persistent_max_m() &&
+        return use_cluster && !cta_eligible(L) && (int64_t)L.n <= cluster_max_n() && (int64_t)L.m <= cluster_max_m() &&
                k <= WARP_TABLE &&
                coop_smem() + coop_static_smem() <= (size_t)device_info().max_smem_optin && cluster_size() > 0;
     }
@@ -938,7 +951,7 @@ struct Refiner {
         RebArgs<O, W> rbw = reb_args(L, weak_max_dest(pb.size_max), pb.opt, pb.size_max, false);
         RebArgs<O, W> rbs = reb_args(L, strong_max_dest(pb.opt, pb.size_max), pb.opt, pb.size_max, false);
         CoopScratch<O, E, W> cs{cbar.p, cwsum.p, chist.p, sk0.p, sk1.p, sv0.p, sv1.p, wpre.p, cmarked.p, coop_qcap(),
-                                coop_boff_cap()};
+                                coop_boff_cap(), (int64_t)coop_boff_off()};
         int bits = bits_for((uint64_t)rbw.none_key);
         int max_iters = 1 << 22;
         RefArgs<O, E, W> a = args(L);
