@@ -613,7 +613,13 @@ void jet_thread_batch_mode(int on) {
     // one CTA for small levels, a 16-CTA cluster for mid-size ones (it needs
     // 16 SMs, not the whole GPU), the host loop above; the loops' options
     // (state in shared memory, the rebalance queue) as everywhere else
-    t_driver_mask = on ? (JET_DRIVER_CTA | JET_DRIVER_CLUSTER | JET_DRIVER_CTA_SMEM | JET_DRIVER_REB_QUEUE) : JET_DRIVER_ALL;
+    // (JET_BATCH_DRIVERS, read once per process, replaces this mask for tuning)
+    static const int batch_mask = [] {
+        const char* v = std::getenv("JET_BATCH_DRIVERS");
+        return (v && *v) ? (std::atoi(v) & JET_DRIVER_ALL)
+                         : (JET_DRIVER_CTA | JET_DRIVER_CLUSTER | JET_DRIVER_CTA_SMEM | JET_DRIVER_REB_QUEUE);
+    }();
+    t_driver_mask = on ? batch_mask : JET_DRIVER_ALL;
     t_batch = on != 0;
 }
 
